@@ -1,0 +1,227 @@
+// extern "C" entry points of libever_b200.so (declared in include/ever_b200.h).
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "common.cuh"
+#include "internal.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int cuda_status(cudaError_t e, const char* where) {
+  if (e == cudaSuccess) return EVER_OK;
+  return fail(EVER_ERR_CUDA, "%s: %s", where, cudaGetErrorString(e));
+}
+
+EverTune resolve_tune(const EverTune* t) {
+  EverTune r{};
+  if (t) r = *t;
+  if (r.kbuf != 8 && r.kbuf != 16 && r.kbuf != 32) r.kbuf = 16;
+  if (r.block != 64 && r.block != 128 && r.block != 256) r.block = 128;
+  return r;
+}
+
+int resolve_degree(const EverScene* sc, const EverTraceArgs* a, int* deg) {
+  int d = a->sh_degree;
+  if (d < 0) {
+    int k = 0;
+    while ((k + 1) * (k + 1) <= sc->sh_coeffs) ++k;  // int(sqrt(K)), py_binding.cpp:206
+    d = k - 1;
+  }
+  if (d < 0 || d > 3) return fail(EVER_ERR_INVALID, "sh_degree %d out of range 0..3", d);
+  if ((d + 1) * (d + 1) > sc->sh_coeffs)
+    return fail(EVER_ERR_INVALID, "sh_degree %d needs %d SH coefficients, features have %d", d, (d + 1) * (d + 1),
+                sc->sh_coeffs);
+  *deg = d;
+  return EVER_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ever_last_error(void) { return g_last_error.c_str(); }
+
+int ever_abi_version(void) { return EVER_ABI_VERSION; }
+
+size_t ever_scene_workspace_bytes(int64_t num_prims, int32_t sh_coeffs) {
+  if (num_prims < 0 || sh_coeffs < 1) return 0;
+  return size_t(ever::scene_layout(num_prims, sh_coeffs).total);
+}
+
+int ever_scene_build(const float* mean, const float* scale, const float* quat, const float* density,
+                     const float* features, int64_t num_prims, int32_t sh_coeffs, void* workspace,
+                     size_t workspace_bytes, EverScene* scene, void* stream) {
+  if (!scene) return fail(EVER_ERR_INVALID, "scene is null");
+  if (num_prims < 0 || num_prims >= (int64_t(1) << 30))
+    return fail(EVER_ERR_INVALID, "num_prims %lld out of range [0, 2^30)", (long long)num_prims);
+  if (sh_coeffs < 1 || sh_coeffs > 16) return fail(EVER_ERR_INVALID, "sh_coeffs %d out of range 1..16", sh_coeffs);
+  if (num_prims > 0 && (!mean || !scale || !quat || !density || !features))
+    return fail(EVER_ERR_INVALID, "null ellipsoid parameter pointer");
+  const ever::SceneLayout L = ever::scene_layout(num_prims, sh_coeffs);
+  if (num_prims > 0 && (!workspace || workspace_bytes < size_t(L.total)))
+    return fail(EVER_ERR_WORKSPACE, "scene workspace needs %lld bytes, got %zu", (long long)L.total, workspace_bytes);
+  if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0) return fail(EVER_ERR_INVALID, "workspace not 256-byte aligned");
+  cudaError_t e = ever::scene_build(mean, scale, quat, density, features, num_prims, sh_coeffs,
+                                    static_cast<char*>(workspace), L, scene, static_cast<cudaStream_t>(stream));
+  return cuda_status(e, "ever_scene_build");
+}
+
+int ever_scene_set_features(EverScene* scene, const float* features, void* stream) {
+  if (!scene) return fail(EVER_ERR_INVALID, "scene is null");
+  if (scene->num_prims > 0 && !features) return fail(EVER_ERR_INVALID, "features is null");
+  return cuda_status(ever::scene_set_features(scene, features, static_cast<cudaStream_t>(stream)),
+                     "ever_scene_set_features");
+}
+
+int ever_trace_forward(const EverScene* scene, const float* rayo, const float* rayd, int64_t num_rays,
+                       const EverTraceArgs* args, const int32_t* ray_order, const EverTune* tune,
+                       const EverForwardOut* out, void* stream) {
+  if (!scene || !args || !out) return fail(EVER_ERR_INVALID, "null scene, args or out");
+  if (num_rays < 0 || num_rays >= (int64_t(1) << 40)) return fail(EVER_ERR_INVALID, "num_rays out of range");
+  if (num_rays > 0 && (!rayo || !rayd || !out->out || !out->iters))
+    return fail(EVER_ERR_INVALID, "null rayo, rayd, out or iters");
+  if (out->event_log && out->log_cap < 0) return fail(EVER_ERR_INVALID, "negative log_cap");
+  int deg = 0;
+  if (int rc = resolve_degree(scene, args, &deg)) return rc;
+  ever::FwdParams P{};
+  P.nodes = scene->nodes;
+  P.records = scene->records;
+  P.features = scene->features;
+  P.order = scene->order;
+  P.N = scene->num_prims;
+  P.K = scene->sh_coeffs;
+  P.rayo = rayo;
+  P.rayd = rayd;
+  P.R = num_rays;
+  P.tmin = args->tmin;
+  P.tmax = args->tmax;
+  P.max_iters = args->max_iters;
+  P.ray_order = ray_order;
+  P.out = *out;
+  return cuda_status(ever::launch_forward(P, deg, resolve_tune(tune), static_cast<cudaStream_t>(stream)),
+                     "ever_trace_forward");
+}
+
+size_t ever_backward_workspace_bytes(int64_t num_prims, int32_t sh_coeffs) {
+  if (num_prims < 0 || sh_coeffs < 1) return 0;
+  ever::WsCursor c;
+  c.take(num_prims * 16 * sizeof(float));
+  c.take(num_prims * int64_t(ever::feat_stride(sh_coeffs)) * sizeof(float));
+  return size_t(c.offset);
+}
+
+int ever_trace_backward(const EverScene* scene, const float* rayo, const float* rayd, int64_t num_rays,
+                        const EverTraceArgs* args, const float* grad_out, const float* states,
+                        const int32_t* iters, const int32_t* event_log, int32_t log_cap, const float* wct,
+                        int32_t num_wct, const float* mean, const float* scale, const float* quat, void* workspace,
+                        size_t workspace_bytes, const int32_t* ray_order, const EverTune* tune,
+                        const EverBackwardOut* out, void* stream) {
+  if (!scene || !args || !out) return fail(EVER_ERR_INVALID, "null scene, args or out");
+  const int64_t N = scene->num_prims;
+  if (num_rays < 0) return fail(EVER_ERR_INVALID, "num_rays out of range");
+  if (num_rays > 0 && (!rayo || !rayd || !grad_out || !states || !iters || !event_log || !out->drayo || !out->drayd))
+    return fail(EVER_ERR_INVALID, "null ray-side pointer");
+  if (N > 0 && (!mean || !scale || !quat || !out->dmean || !out->dscale || !out->dquat || !out->ddensity ||
+                !out->dfeatures))
+    return fail(EVER_ERR_INVALID, "null ellipsoid-side pointer");
+  if (log_cap < args->max_iters - 1 && num_rays > 0)
+    return fail(EVER_ERR_INVALID, "event log holds %d rows, backward needs max_iters-1 = %d", log_cap,
+                args->max_iters - 1);
+  if (wct && num_wct < 1) return fail(EVER_ERR_INVALID, "wct given with num_wct < 1");
+  int deg = 0;
+  if (int rc = resolve_degree(scene, args, &deg)) return rc;
+  const size_t need = ever_backward_workspace_bytes(N, scene->sh_coeffs);
+  if (N > 0 && (!workspace || workspace_bytes < need))
+    return fail(EVER_ERR_WORKSPACE, "backward workspace needs %zu bytes, got %zu", need, workspace_bytes);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  ever::WsCursor c;
+  char* ws = static_cast<char*>(workspace);
+  float* acc_geo = reinterpret_cast<float*>(ws + c.take(N * 16 * sizeof(float)));
+  float* acc_feat = reinterpret_cast<float*>(ws + c.take(N * int64_t(ever::feat_stride(scene->sh_coeffs)) * sizeof(float)));
+  cudaError_t e = cudaSuccess;
+  if (N > 0) e = cudaMemsetAsync(workspace, 0, need, st);
+  if (e != cudaSuccess) return cuda_status(e, "ever_trace_backward memset");
+  const bool per_ray_wct = wct && num_wct > 1 && out->dmeans2d;
+  if (per_ray_wct && N > 0) {
+    e = cudaMemsetAsync(out->dmeans2d, 0, N * 2 * sizeof(float), st);
+    if (e != cudaSuccess) return cuda_status(e, "ever_trace_backward memset");
+  }
+  const EverTune tn = resolve_tune(tune);
+  if (N > 0) {
+    ever::BwdParams P{};
+    P.nodes = scene->nodes;
+    P.records = scene->records;
+    P.features = scene->features;
+    P.order = scene->order;
+    P.N = N;
+    P.K = scene->sh_coeffs;
+    P.rayo = rayo;
+    P.rayd = rayd;
+    P.R = num_rays;
+    P.tmin = args->tmin;
+    P.tmax = args->tmax;
+    P.max_iters = args->max_iters;
+    P.ray_order = ray_order;
+    P.grad_out = grad_out;
+    P.states = states;
+    P.iters = iters;
+    P.event_log = event_log;
+    P.log_cap = log_cap;
+    P.wct = wct;
+    P.num_wct = num_wct;
+    P.acc_geo = acc_geo;
+    P.acc_feat = acc_feat;
+    P.dmeans2d = out->dmeans2d;
+    P.drayo = out->drayo;
+    P.drayd = out->drayd;
+    e = ever::launch_backward(P, deg, tn, st);
+    if (e != cudaSuccess) return cuda_status(e, "ever_trace_backward");
+    ever::FinalizeParams F{};
+    F.records = scene->records;
+    F.order = scene->order;
+    F.N = N;
+    F.K = scene->sh_coeffs;
+    F.mean = mean;
+    F.scale = scale;
+    F.quat = quat;
+    F.acc_geo = acc_geo;
+    F.acc_feat = acc_feat;
+    F.wct = wct;
+    F.num_wct = wct ? num_wct : 0;
+    F.out = *out;
+    e = ever::launch_finalize(F, st);
+    return cuda_status(e, "ever_trace_backward finalize");
+  }
+  // no ellipsoids: every ray gradient is zero
+  if (num_rays > 0) {
+    e = cudaMemsetAsync(out->drayo, 0, num_rays * 3 * sizeof(float), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(out->drayd, 0, num_rays * 3 * sizeof(float), st);
+  }
+  return cuda_status(e, "ever_trace_backward");
+}
+
+int ever_event_log_to_reference(const EverScene* scene, const int32_t* event_log, int32_t log_cap,
+                                const int32_t* iters, int64_t num_rays, int32_t* tri_collection, int32_t max_iters,
+                                void* stream) {
+  if (!scene || (num_rays > 0 && max_iters > 0 && (!event_log || !iters || !tri_collection)))
+    return fail(EVER_ERR_INVALID, "null pointer");
+  return cuda_status(ever::launch_log_to_reference(scene->order, event_log, log_cap, iters, num_rays, tri_collection,
+                                                   max_iters, static_cast<cudaStream_t>(stream)),
+                     "ever_event_log_to_reference");
+}
+
+}  // extern "C"

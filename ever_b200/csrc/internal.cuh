@@ -1,0 +1,102 @@
+// Host-side internals shared by the translation units of libever_b200.
+#pragma once
+
+#include <algorithm>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "ever_b200.h"
+
+namespace ever {
+
+// Bump allocator over a caller-provided workspace: 256-byte aligned segments.
+struct WsCursor {
+  int64_t offset = 0;
+  int64_t take(int64_t bytes) {
+    const int64_t at = offset;
+    offset += (std::max<int64_t>(bytes, 0) + 255) / 256 * 256;
+    return at;
+  }
+};
+
+struct SceneLayout {
+  int64_t nodes, records, features, order;
+  int64_t aabb_a, aabb_b, keys_a, keys_b, vals_a, vals_b, hist;
+  int64_t parent_node, parent_leaf, flags, bounds;
+  int nblocks;
+  int64_t total;
+};
+
+SceneLayout scene_layout(int64_t N, int K);
+cudaError_t scene_build(const float* mean, const float* scale, const float* quat, const float* density,
+                        const float* feat, int64_t N, int K, char* ws, const SceneLayout& L, EverScene* sc,
+                        cudaStream_t st);
+cudaError_t scene_set_features(EverScene* sc, const float* feat, cudaStream_t st);
+
+struct FwdParams {
+  const void* nodes;
+  const void* records;
+  const float* features;
+  const int32_t* order;
+  int64_t N;
+  int K;
+  const float* rayo;
+  const float* rayd;
+  int64_t R;
+  float tmin, tmax;
+  int max_iters;
+  const int32_t* ray_order;
+  EverForwardOut out;
+};
+
+cudaError_t launch_forward(const FwdParams& P, int deg, const EverTune& tune, cudaStream_t st);
+
+struct BwdParams {
+  const void* nodes;
+  const void* records;
+  const float* features;
+  const int32_t* order;
+  int64_t N;
+  int K;
+  const float* rayo;
+  const float* rayd;
+  int64_t R;
+  float tmin, tmax;
+  int max_iters;
+  const int32_t* ray_order;
+  const float* grad_out;
+  const float* states;
+  const int32_t* iters;
+  const int32_t* event_log;
+  int log_cap;
+  const float* wct;
+  int num_wct;
+  float* acc_geo;   // N x 16 (W 9, mean 3, density 1, pad 3), Morton order
+  float* acc_feat;  // N x K x 3, Morton order
+  float* dmeans2d;  // per-ray wct mode accumulates here directly (original order)
+  float* drayo;
+  float* drayd;
+};
+
+cudaError_t launch_backward(const BwdParams& P, int deg, const EverTune& tune, cudaStream_t st);
+
+struct FinalizeParams {
+  const void* records;
+  const int32_t* order;
+  int64_t N;
+  int K;
+  const float* mean;
+  const float* scale;
+  const float* quat;
+  const float* acc_geo;
+  const float* acc_feat;
+  const float* wct;  // first matrix, for the single-camera dmeans2d
+  int num_wct;
+  EverBackwardOut out;
+};
+
+cudaError_t launch_finalize(const FinalizeParams& P, cudaStream_t st);
+cudaError_t launch_log_to_reference(const int32_t* order, const int32_t* log, int log_cap, const int32_t* iters,
+                                    int64_t R, int32_t* tri, int max_iters, cudaStream_t st);
+
+}  // namespace ever

@@ -1,0 +1,142 @@
+"""Drop-in for splinetracers.fast_ellipsoid_splinetracer (N-Demir/ever).
+
+Same entry point, arguments, output layout and autograd behaviour as
+splinetracers/fast_ellipsoid_splinetracer.py:37-256:
+
+    trace_rays(mean, scale, quat, density, features, rayo, rayd, tmin=0.0, tmax=1000,
+               max_prim_size=3, dL_dmeans2D=None, wcts=None, max_iters=500,
+               return_extras=False)
+    -> (R,5) [R, G, B, opacity, distortion]  (or (out, extras) with return_extras)
+
+`trace_rays.uses_density` is True, as callers test it (ever.py:184). The backward
+returns the 14 gradient slots of SplineTracer.backward (:204-219) with the same
+clipping. Everything runs in libever_b200.so: an LBVH built on the device per call
+(the reference rebuilds its GAS per call as well, :66-71), a CUDA traversal/integration
+kernel and a CUDA reverse-replay backward.
+
+Colour: the SH degree is sqrt(K)-1 of features (N,K,3) as in py_binding.cpp:206 and the
+colour of each ellipsoid is evaluated along the ray direction rayd, as the reference's
+backward evaluates it (backwards_kernel.slang:162, 238). At degree 0 (the trainer's
+case) this equals the reference's forward, which reads only the DC term; pass
+sh_degree=0 to get that DC-only colour with higher-degree features too.
+"""
+from __future__ import annotations
+
+from typing import Any
+
+import torch
+from torch.autograd import Function
+
+from . import tracer as T
+
+__all__ = ["SplineTracer", "trace_rays", "SavedForBackward"]
+
+
+class SavedForBackward:
+    """Mirror of the reference's fesSavedForBackward (py_binding.cpp:151-193)."""
+
+    def __init__(self, states, diracs, iters, touch_count, faces=None):
+        self.states = states
+        self.diracs = diracs
+        self.iters = iters
+        self.touch_count = touch_count
+        self.faces = faces if faces is not None else torch.zeros_like(iters)
+
+
+class SplineTracer(Function):
+    @staticmethod
+    def forward(
+        ctx: Any,
+        mean: torch.Tensor,
+        scale: torch.Tensor,
+        quat: torch.Tensor,
+        density: torch.Tensor,
+        color: torch.Tensor,
+        rayo: torch.Tensor,
+        rayd: torch.Tensor,
+        tmin: float,
+        tmax: float,
+        max_prim_size: float,
+        mean2D: torch.Tensor,
+        wcts: torch.Tensor,
+        max_iters: int,
+        return_extras: bool = False,
+        sh_degree: int | None = None,
+        tune: T.Tune | None = None,
+    ):
+        ctx.device = rayo.device
+        scene = T.Scene(mean, scale, quat, density, color)
+        needs_grad = any(ctx.needs_input_grad[:7]) or (mean2D is not None and ctx.needs_input_grad[10])
+        fwd = T.forward(scene, rayo, rayd, tmin, tmax, max_iters, sh_degree,
+                        log_events=needs_grad or return_extras, touch_count=return_extras, tune=tune)
+        ctx.scene = scene
+        ctx.fwd = fwd
+        ctx.tmin, ctx.tmax, ctx.max_iters = tmin, tmax, max_iters
+        ctx.max_prim_size = max_prim_size
+        ctx.sh_degree = sh_degree
+        ctx.tune = tune
+        ctx.has_wcts = wcts is not None
+        ctx.density_shape = density.shape
+        ctx.save_for_backward(rayo, rayd, wcts)
+        out = fwd.out
+        if return_extras:
+            saved = SavedForBackward(fwd.states, fwd.last_dirac, fwd.iters, fwd.touch_count)
+            return out, dict(
+                tri_collection=T.reference_tri_collection(scene, fwd, max_iters) if fwd.event_log is not None
+                else torch.zeros(rayo.shape[0] * max_iters, dtype=torch.int32, device=rayo.device),
+                iters=fwd.iters,
+                opacity=out[:, 3],
+                touch_count=fwd.touch_count,
+                distortion_loss=out[:, 4],
+                saved=saved,
+            )
+        return out
+
+    @staticmethod
+    def backward(ctx, grad_output: torch.Tensor, *unused):
+        rayo, rayd, wcts = ctx.saved_tensors
+        g = T.backward(ctx.scene, rayo, rayd, ctx.fwd, grad_output, ctx.tmin, ctx.tmax, ctx.max_iters,
+                       ctx.sh_degree, wcts=wcts, want_means2d=ctx.has_wcts, tune=ctx.tune)
+        return (
+            g.mean,
+            g.scale,
+            g.quat,
+            g.density.reshape(ctx.density_shape),
+            g.features,
+            g.rayo,
+            g.rayd,
+            None,
+            None,
+            None,
+            g.means2d,
+            None,
+            None,
+            None,
+            None,
+            None,
+        )
+
+
+def trace_rays(
+    mean: torch.Tensor,
+    scale: torch.Tensor,
+    quat: torch.Tensor,
+    density: torch.Tensor,
+    features: torch.Tensor,
+    rayo: torch.Tensor,
+    rayd: torch.Tensor,
+    tmin: float = 0.0,
+    tmax: float = 1000,
+    max_prim_size: float = 3,
+    dL_dmeans2D=None,
+    wcts=None,
+    max_iters: int = 500,
+    return_extras: bool = False,
+    sh_degree: int | None = None,
+    tune: T.Tune | None = None,
+):
+    return SplineTracer.apply(mean, scale, quat, density, features, rayo, rayd, tmin, tmax, max_prim_size,
+                              dL_dmeans2D, wcts, max_iters, return_extras, sh_degree, tune)
+
+
+trace_rays.uses_density = True

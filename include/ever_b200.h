@@ -1,0 +1,152 @@
+/* C ABI of the B200-native exact volumetric ellipsoid tracer (libever_b200.so).
+ *
+ * Drop-in replacement for the native layer under EVER's Python API
+ * splinetracers/fast_ellipsoid_splinetracer.py:222-256 (trace_rays). In the
+ * reference that layer is a pybind11 module (splinetracers/fast_ellipsoid_splinetracer/
+ * py_binding.cpp:261-282) over OptiX plus two slangtorch kernels; here it is plain C:
+ * device pointers and sizes in, status code out, message via ever_last_error().
+ *
+ * Conventions
+ *  - All float/int pointers are DEVICE pointers (CUDA global memory) unless noted.
+ *  - `stream` is a cudaStream_t passed as void*; NULL means the legacy default stream.
+ *  - No function allocates device memory, synchronises the host, or throws: callers
+ *    pass workspaces sized by the *_workspace_bytes() functions, and every call only
+ *    enqueues kernels on `stream`, so the calls can be captured in a CUDA graph.
+ *  - Return value: EVER_OK (0) or an EVER_ERR_* code; ever_last_error() then holds a
+ *    message (thread-local).
+ *  - Ellipsoid parameters follow the reference: mean (N,3), scale (N,3), quat (N,4)
+ *    as (r,x,y,z) and not required to be unit, density (N), features (N,K,3) SH
+ *    coefficients, all fp32 contiguous.
+ */
+#ifndef EVER_B200_H
+#define EVER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EVER_OK 0
+#define EVER_ERR_INVALID 1   /* bad argument (shape, null pointer, size) */
+#define EVER_ERR_CUDA 2      /* a CUDA launch or API call failed */
+#define EVER_ERR_WORKSPACE 3 /* workspace too small */
+
+#define EVER_ABI_VERSION 1
+
+/* A scene built by ever_scene_build(): a binary LBVH over the ellipsoids plus their
+ * intersection records, both in Morton order, all inside the caller's workspace.
+ * Replaces the reference's Primitives + GAS objects (py_binding.cpp:94-149,
+ * GAS.cpp:56-154, create_aabbs.cu:69-132). Plain data: may be copied by value. */
+typedef struct EverScene {
+  int64_t num_prims;  /* N */
+  int32_t sh_coeffs;  /* K: SH coefficients stored per ellipsoid (feature stride) */
+  int32_t num_nodes;  /* internal BVH nodes: max(N-1, 1), 0 if N == 0 */
+  void* nodes;        /* num_nodes x 64 B: child boxes + child links */
+  void* records;      /* N x 64 B: 3x3 local-frame matrix, mean, density, index */
+  float* features;    /* N rows of 3K floats padded to a multiple of 4, Morton order */
+  int32_t* order;     /* N: Morton position -> original ellipsoid index */
+  void* scratch;      /* build-time scratch inside the workspace */
+} EverScene;
+
+/* Launch configuration chosen by the autotuner (0 = built-in default). */
+typedef struct EverTune {
+  int32_t kbuf;       /* events gathered per traversal round: 8, 16 or 32 */
+  int32_t block;      /* threads per block: 64, 128 or 256 */
+  int32_t traversal;  /* 0: warp packets share one node walk (default); 1: one walk per ray */
+  int32_t reserved[5];
+} EverTune;
+
+/* Per-ray outputs of a forward trace. Null pointers are skipped unless noted. */
+typedef struct EverForwardOut {
+  float* out;          /* (R,5) RGB, opacity, distortion (required) */
+  float* states;       /* (R,16) final SplineState (structs.h:41-53 layout); needed by backward */
+  float* last_dirac;   /* (R,4) dirac of the last consumed event */
+  int32_t* iters;      /* (R) consumed events (required) */
+  int32_t* event_log;  /* (log_cap, R) iteration-major event ids in Morton numbering
+                          (2j+1 entry, 2j exit); needed by backward */
+  int32_t log_cap;     /* rows of event_log (>= max_iters to log every event) */
+  int32_t* touch_count;/* (N) original order: events per ellipsoid (atomic, exact) */
+  float* ray_stats;    /* (R,2): consumed events, termination depth (t of last event) */
+  int32_t* status;     /* (1) OR of EVER_STATUS_* flags raised by the kernels */
+} EverForwardOut;
+
+#define EVER_STATUS_STACK_OVERFLOW 1
+#define EVER_STATUS_LOG_OVERFLOW 2
+#define EVER_STATUS_INIT_OVERFLOW 4
+
+/* Gradients of a backward trace. Prim gradients are written in original order and
+ * clipped as fast_ellipsoid_splinetracer.py:204-219 clips them. */
+typedef struct EverBackwardOut {
+  float* dmean;      /* (N,3) */
+  float* dscale;     /* (N,3) */
+  float* dquat;      /* (N,4) */
+  float* ddensity;   /* (N) */
+  float* dfeatures;  /* (N,K,3) */
+  float* drayo;      /* (R,3) */
+  float* drayd;      /* (R,3) */
+  float* dmeans2d;   /* (N,2) or NULL; needs wct */
+} EverBackwardOut;
+
+typedef struct EverTraceArgs {
+  float tmin;
+  float tmax;
+  int32_t max_iters;
+  int32_t sh_degree;  /* SH degree evaluated (0..3); -1: sqrt(K)-1 as py_binding.cpp:206 */
+} EverTraceArgs;
+
+const char* ever_last_error(void);
+int ever_abi_version(void);
+
+/* Bytes of workspace ever_scene_build() needs for N ellipsoids with K SH coefficients. */
+size_t ever_scene_workspace_bytes(int64_t num_prims, int32_t sh_coeffs);
+
+/* Builds the scene: AABBs of the ellipsoids (create_aabbs.cu:69-115), 30-bit Morton
+ * codes, an on-device LSD radix sort, a Karras LBVH and a bottom-up box refit; then
+ * reorders records and features into Morton order. Replaces Primitives.add_primitives
+ * + GAS (py_binding.cpp:99-132, GAS.cpp:56-154). */
+int ever_scene_build(const float* mean, const float* scale, const float* quat, const float* density,
+                     const float* features, int64_t num_prims, int32_t sh_coeffs, void* workspace,
+                     size_t workspace_bytes, EverScene* scene, void* stream);
+
+/* Replaces the features of a built scene (same N and K) without rebuilding the BVH.
+ * Counterpart of Primitives.set_features + Forward.update_model (py_binding.cpp:133-138, 207-209). */
+int ever_scene_set_features(EverScene* scene, const float* features, void* stream);
+
+/* Forward trace of R rays: rayo/rayd (R,3). Counterpart of Forward.trace_rays
+ * (py_binding.cpp:210-258, Forward.cpp:23-82, shaders.slang:171-235), including the
+ * initial density of rays that start inside ellipsoids (initialize_density.cu:152-208).
+ * ray_order (R, nullable): the order in which threads pick rays up (a permutation);
+ * results are written by ray index and do not depend on it. */
+int ever_trace_forward(const EverScene* scene, const float* rayo, const float* rayd, int64_t num_rays,
+                       const EverTraceArgs* args, const int32_t* ray_order, const EverTune* tune,
+                       const EverForwardOut* out, void* stream);
+
+/* Bytes of gradient-accumulation workspace ever_trace_backward() needs. */
+size_t ever_backward_workspace_bytes(int64_t num_prims, int32_t sh_coeffs);
+
+/* Backward of a forward trace: grad_out (R,5); states/iters/event_log from the forward.
+ * Counterpart of SplineTracer.backward (fast_ellipsoid_splinetracer.py:106-219) with
+ * backwards_kernel and backwards_initial_drgb_kernel (backwards_kernel.slang:259-428).
+ * wct (4x4 row-major, nullable) with num_wct matrices: ray r uses wct[r] if r < num_wct,
+ * else wct[0], for dmeans2d as backwards_kernel.slang:313-321. */
+int ever_trace_backward(const EverScene* scene, const float* rayo, const float* rayd, int64_t num_rays,
+                        const EverTraceArgs* args, const float* grad_out, const float* states,
+                        const int32_t* iters, const int32_t* event_log, int32_t log_cap,
+                        const float* wct, int32_t num_wct, const float* mean, const float* scale,
+                        const float* quat, void* workspace, size_t workspace_bytes,
+                        const int32_t* ray_order, const EverTune* tune, const EverBackwardOut* out,
+                        void* stream);
+
+/* Converts an event log in Morton numbering into the reference's tri_collection ids
+ * (2p+1 entry, 2p exit with original indices p; fast_ellipsoid_splinetracer.py:93-101).
+ * Entries at or beyond iters[r] are set to 0, as the reference's zero-filled buffer. */
+int ever_event_log_to_reference(const EverScene* scene, const int32_t* event_log, int32_t log_cap,
+                                const int32_t* iters, int64_t num_rays, int32_t* tri_collection,
+                                int32_t max_iters, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EVER_B200_H */

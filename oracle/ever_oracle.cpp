@@ -196,31 +196,31 @@ template <class T> inline void sh_basis(const T dir[3], int deg, T B[16]) {
 }
 
 // d B_k / d(x,y,z) (rows k, cols xyz), double only.
-inline void sh_basis_grad(const double dir[3], int deg, double J[16][3]) {
-  const double x = dir[0], y = dir[1], z = dir[2];
+template <class T> inline void sh_basis_grad(const T dir[3], int deg, T J[16][3]) {
+  const T x = dir[0], y = dir[1], z = dir[2];
   for (int k = 0; k < 16; ++k) J[k][0] = J[k][1] = J[k][2] = 0;
   if (deg < 1) return;
-  const double C1 = K<double>::c1;
+  const T C1 = K<T>::c1;
   J[1][1] = -C1;
   J[2][2] = C1;
   J[3][0] = -C1;
   if (deg < 2) return;
-  const double* C2 = K<double>::c2;
+  const T* C2 = K<T>::c2;
   J[4][0] = C2[0] * y; J[4][1] = C2[0] * x;
   J[5][1] = C2[1] * z; J[5][2] = C2[1] * y;
-  J[6][0] = -2 * C2[2] * x; J[6][1] = -2 * C2[2] * y; J[6][2] = 4 * C2[2] * z;
+  J[6][0] = -T(2) * C2[2] * x; J[6][1] = -T(2) * C2[2] * y; J[6][2] = T(4) * C2[2] * z;
   J[7][0] = C2[3] * z; J[7][2] = C2[3] * x;
-  J[8][0] = 2 * C2[4] * x; J[8][1] = -2 * C2[4] * y;
+  J[8][0] = T(2) * C2[4] * x; J[8][1] = -T(2) * C2[4] * y;
   if (deg < 3) return;
-  const double* C3 = K<double>::c3;
-  const double xx = x * x, yy = y * y, zz = z * z;
-  J[9][0] = 6 * C3[0] * x * y; J[9][1] = C3[0] * (3 * xx - 3 * yy);
+  const T* C3 = K<T>::c3;
+  const T xx = x * x, yy = y * y, zz = z * z;
+  J[9][0] = T(6) * C3[0] * x * y; J[9][1] = C3[0] * (3 * xx - 3 * yy);
   J[10][0] = C3[1] * y * z; J[10][1] = C3[1] * x * z; J[10][2] = C3[1] * x * y;
-  J[11][0] = -2 * C3[2] * x * y; J[11][1] = C3[2] * (4 * zz - xx - 3 * yy); J[11][2] = 8 * C3[2] * y * z;
-  J[12][0] = -6 * C3[3] * x * z; J[12][1] = -6 * C3[3] * y * z; J[12][2] = C3[3] * (6 * zz - 3 * xx - 3 * yy);
-  J[13][0] = C3[4] * (4 * zz - 3 * xx - yy); J[13][1] = -2 * C3[4] * x * y; J[13][2] = 8 * C3[4] * x * z;
-  J[14][0] = 2 * C3[5] * x * z; J[14][1] = -2 * C3[5] * y * z; J[14][2] = C3[5] * (xx - yy);
-  J[15][0] = C3[6] * (3 * xx - 3 * yy); J[15][1] = -6 * C3[6] * x * y;
+  J[11][0] = -T(2) * C3[2] * x * y; J[11][1] = C3[2] * (4 * zz - xx - 3 * yy); J[11][2] = T(8) * C3[2] * y * z;
+  J[12][0] = -T(6) * C3[3] * x * z; J[12][1] = -T(6) * C3[3] * y * z; J[12][2] = C3[3] * (6 * zz - 3 * xx - 3 * yy);
+  J[13][0] = C3[4] * (4 * zz - 3 * xx - yy); J[13][1] = -T(2) * C3[4] * x * y; J[13][2] = T(8) * C3[4] * x * z;
+  J[14][0] = T(2) * C3[5] * x * z; J[14][1] = -T(2) * C3[5] * y * z; J[14][2] = C3[5] * (xx - yy);
+  J[15][0] = C3[6] * (3 * xx - 3 * yy); J[15][1] = -T(6) * C3[6] * x * y;
 }
 
 template <class T> struct State {  // SplineState, spline-machine.slang:20-32
@@ -444,30 +444,54 @@ int trace_impl(int64_t N, int Kc, int deg, const S* mean, const S* scale, const 
   return 0;
 }
 
-// ---------------------------------------------------------------- FP64 backward
-struct Grad {
-  std::vector<double> W, mu, sigma, feat;  // per ellipsoid (W: 9 per ellipsoid)
+// ---------------------------------------------------------------- backward
+// FP64: exact analytic gradients along a fixed event sequence, states stored from a
+// forward replay. FP32 with inverse_replay: the reference's own scheme
+// (backwards_kernel.slang:327-361): states recovered from the final state by
+// inverse_update_dual (spline-machine.slang:65-100), in float, as the CUDA kernel does.
+template <class T> struct Grad {
+  std::vector<T> W, mu, sigma, feat;  // per ellipsoid (W: 9 per ellipsoid)
 };
 
-// VJP of update() (double), cotangent G of the new state -> cotangent of the old
+// VJP of update() (T), cotangent G of the new state -> cotangent of the old
 // state (Gs) and of the control point (Gt, Gdirac). Clamps pass the gradient only
 // strictly inside their range.
-inline void update_vjp(const State<double>& s, double t, const State<double>& G, State<double>& Gs,
-                       double& Gt, double Gdirac[4]) {
-  const double dt_raw = t - s.t;
-  const double dt = std::fmax(dt_raw, 0.0);
-  const double area_raw = s.drgb[0] * dt;
-  const double area = std::fmax(area_raw, 0.0);
-  double rgb[3];
+// inverse_update_dual, spline-machine.slang:65-100 (same operation order as the CUDA kernel).
+template <class T> inline State<T> inverse_update(const State<T>& n, const T dirac_new[4], T t_old) {
+  State<T> s;
+  const T dt = fmx(n.t - t_old, T(0));
+  for (int i = 0; i < 4; ++i) s.drgb[i] = n.drgb[i] - dirac_new[i];
+  s.t = t_old;
+  const T area = fmx(s.drgb[0] * dt, T(0));
+  T rgb[3];
   for (int i = 0; i < 3; ++i) rgb[i] = safe_div(s.drgb[1 + i], s.drgb[0]);
-  const double ea_in = -area, el_in = -s.logT;
-  const double e1 = safe_exp(ea_in), e2 = safe_exp(el_in);
-  const double wraw = (1.0 - e1) * e2;
-  const double w = clampv(wraw, 0.0, 1.0);
-  const double mid = ((t + s.t) * 0.5) * 1000.0;
-  const double m = tukey(mid);
+  s.logT = fmx(n.logT - area, T(0));
+  const T w = clampv((T(1) - safe_exp(-area)) * safe_exp(-s.logT), T(0), T(1));
+  for (int i = 0; i < 3; ++i) s.C[i] = n.C[i] - w * rgb[i];
+  const T m = tukey(((n.t + s.t) * T(0.5)) * T(1000));
+  s.cum[0] = n.cum[0] - w;
+  s.cum[1] = n.cum[1] - w * m;
+  s.dist[0] = n.dist[0] - T(2) * w * m * s.cum[0];
+  s.dist[1] = n.dist[1] - T(2) * w * s.cum[1];
+  return s;
+}
 
-  Gs = State<double>();
+template <class T>
+inline void update_vjp(const State<T>& s, T t, const State<T>& G, State<T>& Gs, T& Gt, T Gdirac[4]) {
+  const T dt_raw = t - s.t;
+  const T dt = std::fmax(dt_raw, T(0));
+  const T area_raw = s.drgb[0] * dt;
+  const T area = std::fmax(area_raw, T(0));
+  T rgb[3];
+  for (int i = 0; i < 3; ++i) rgb[i] = safe_div(s.drgb[1 + i], s.drgb[0]);
+  const T ea_in = -area, el_in = -s.logT;
+  const T e1 = safe_exp(ea_in), e2 = safe_exp(el_in);
+  const T wraw = (T(1) - e1) * e2;
+  const T w = clampv(wraw, T(0), T(1));
+  const T mid = ((t + s.t) * T(0.5)) * T(1000);
+  const T m = tukey(mid);
+
+  Gs = State<T>();
   // pass-through terms
   for (int i = 0; i < 2; ++i) Gs.dist[i] = G.dist[i];
   for (int i = 0; i < 3; ++i) Gs.C[i] = G.C[i];
@@ -477,47 +501,47 @@ inline void update_vjp(const State<double>& s, double t, const State<double>& G,
   }
   Gt = G.t;
   // logT' = max(area + logT, 0)
-  double g_area = 0.0;
+  T g_area = T(0);
   if (area + s.logT > 0) {
     g_area += G.logT;
     Gs.logT += G.logT;
   }
   // w usage
-  double g_w = 0.0, g_m = 0.0;
+  T g_w = T(0), g_m = T(0);
   for (int i = 0; i < 3; ++i) g_w += G.C[i] * rgb[i];
-  g_w += G.dist[0] * 2.0 * m * s.cum[0] + G.dist[1] * 2.0 * s.cum[1] + G.cum[0] + G.cum[1] * m;
-  g_m += G.dist[0] * 2.0 * w * s.cum[0] + G.cum[1] * w;
-  Gs.cum[0] = G.cum[0] + G.dist[0] * 2.0 * w * m;
-  Gs.cum[1] = G.cum[1] + G.dist[1] * 2.0 * w;
+  g_w += G.dist[0] * T(2) * m * s.cum[0] + G.dist[1] * T(2) * s.cum[1] + G.cum[0] + G.cum[1] * m;
+  g_m += G.dist[0] * T(2) * w * s.cum[0] + G.cum[1] * w;
+  Gs.cum[0] = G.cum[0] + G.dist[0] * T(2) * w * m;
+  Gs.cum[1] = G.cum[1] + G.dist[1] * T(2) * w;
   // rgb = safe_div(drgb_i, drgb_x), custom backward of safe-math.slang:68-80
   for (int i = 0; i < 3; ++i) {
-    const double R = G.C[i] * w;
-    const double a = s.drgb[1 + i], b = s.drgb[0];
-    const double da = std::fabs(b) < K<double>::tiny ? clampv(R / K<double>::tiny, K<double>::minv, K<double>::maxv)
-                                                      : clampv(R / b, K<double>::minv, K<double>::maxv);
-    const double b2 = b * b;
-    const double db = b2 < K<double>::tiny ? clampv(-a / K<double>::tiny * R, K<double>::minv, K<double>::maxv)
-                                           : clampv(-a / b2 * R, K<double>::minv, K<double>::maxv);
+    const T R = G.C[i] * w;
+    const T a = s.drgb[1 + i], b = s.drgb[0];
+    const T da = std::fabs(b) < K<T>::tiny ? clampv(R / K<T>::tiny, K<T>::minv, K<T>::maxv)
+                                                      : clampv(R / b, K<T>::minv, K<T>::maxv);
+    const T b2 = b * b;
+    const T db = b2 < K<T>::tiny ? clampv(-a / K<T>::tiny * R, K<T>::minv, K<T>::maxv)
+                                           : clampv(-a / b2 * R, K<T>::minv, K<T>::maxv);
     Gs.drgb[1 + i] += da;
     Gs.drgb[0] += db;
   }
   // w = clip((1 - e1) * e2, 0, 1)
-  if (wraw > 0.0 && wraw < 1.0) {
-    const double g_wraw = g_w;
-    if (ea_in > K<double>::minv && ea_in < K<double>::logmax) g_area += g_wraw * e2 * e1;  // d(1-e1)/darea = e1
-    if (el_in > K<double>::minv && el_in < K<double>::logmax) Gs.logT += -g_wraw * (1.0 - e1) * e2;
+  if (wraw > T(0) && wraw < T(1)) {
+    const T g_wraw = g_w;
+    if (ea_in > K<T>::minv && ea_in < K<T>::logmax) g_area += g_wraw * e2 * e1;  // d(1-e1)/darea = e1
+    if (el_in > K<T>::minv && el_in < K<T>::logmax) Gs.logT += -g_wraw * (T(1) - e1) * e2;
   }
   // area = max(drgb_x * dt, 0)
-  if (area_raw > 0.0) {
+  if (area_raw > T(0)) {
     Gs.drgb[0] += g_area * dt;
-    const double g_dt = g_area * s.drgb[0];
-    if (dt_raw > 0.0) {
+    const T g_dt = g_area * s.drgb[0];
+    if (dt_raw > T(0)) {
       Gt += g_dt;
       Gs.t -= g_dt;
     }
   }
   // m = tukey(((t + t_s)/2) * 1000)
-  const double g_mid = g_m * dtukey(mid) * 500.0;
+  const T g_mid = g_m * dtukey(mid) * T(500);
   Gt += g_mid;
   Gs.t += g_mid;
 }
@@ -532,35 +556,36 @@ struct BwdOut {
   double* drayd;
 };
 
+template <class T>
 int backward_impl(int64_t N, int Kc, int deg, const double* mean, const double* scale,
                   const double* quat, const double* density, const double* feat, int64_t R,
                   const double* rayo, const double* rayd, double tmin, double tmax, int max_iters,
                   const int32_t* events, const int32_t* iters, const double* dout5, BwdOut out,
-                  int nthreads) {
+                  int nthreads, bool inverse_replay) {
   (void)tmax;
-  Scene<double> sc = make_scene<double>(N, Kc, deg, mean, scale, quat, density, feat);
+  Scene<T> sc = make_scene<T>(N, Kc, deg, mean, scale, quat, density, feat);
   const int nb = (deg + 1) * (deg + 1);
   // per-thread accumulators to stay deterministic per thread; reduced at the end
   nthreads = std::max(1, (int)std::min<int64_t>(nthreads, std::max<int64_t>(R, 1)));
-  std::vector<Grad> acc(nthreads);
+  std::vector<Grad<T>> acc(nthreads);
   for (auto& g : acc) {
-    g.W.assign(9 * N, 0.0);
-    g.mu.assign(3 * N, 0.0);
-    g.sigma.assign(N, 0.0);
-    g.feat.assign((size_t)N * Kc * 3, 0.0);
+    g.W.assign(9 * N, T(0));
+    g.mu.assign(3 * N, T(0));
+    g.sigma.assign(N, T(0));
+    g.feat.assign((size_t)N * Kc * 3, T(0));
   }
-  auto ray_fn = [&](int64_t j, Grad& g) {
+  auto ray_fn = [&](int64_t j, Grad<T>& g) {
     double* gro = out.drayo + 3 * j;
     double* grd = out.drayd + 3 * j;
     for (int i = 0; i < 3; ++i) gro[i] = grd[i] = 0.0;
     const int n = iters[j];
     if (n >= max_iters - 1 || n <= 0) return;  // backwards_kernel.slang:304
-    const double ro[3] = {rayo[3 * j], rayo[3 * j + 1], rayo[3 * j + 2]};
-    const double rd[3] = {rayd[3 * j], rayd[3 * j + 1], rayd[3 * j + 2]};
-    Ray<double> r = make_ray(ro, rd, tmin, deg);
-    // initial density (members recomputed in double)
+    const T ro[3] = {T(rayo[3 * j]), T(rayo[3 * j + 1]), T(rayo[3 * j + 2])};
+    const T rd[3] = {T(rayd[3 * j]), T(rayd[3 * j + 1]), T(rayd[3 * j + 2])};
+    Ray<T> r = make_ray(ro, rd, T(tmin), deg);
+    // initial density (members recomputed in T)
     std::vector<int64_t> members;
-    std::vector<double> ts(n);
+    std::vector<T> ts(n);
     std::vector<int64_t> ps(n);
     std::vector<int> ex(n);
     for (int i = 0; i < n; ++i) {
@@ -568,80 +593,96 @@ int backward_impl(int64_t N, int Kc, int deg, const double* mean, const double* 
       ps[i] = id >> 1;
       ex[i] = (id & 1) ? 0 : 1;
     }
-    State<double> st;
+    State<T> st;
     for (int64_t p = 0; p < N; ++p) {
-      Hit<double> H;
+      Hit<T> H;
       if (intersect(&sc.W[9 * p], &sc.mu[3 * p], r.o, r.d, H) && H.t0 <= 0 && H.t1 > 0) members.push_back(p);
     }
     for (int64_t p : members) {
-      double c[3];
+      T c[3];
       prim_colour(sc, r, p, c);
       st.drgb[0] += sc.sigma[p];
       for (int i = 0; i < 3; ++i) st.drgb[1 + i] += sc.sigma[p] * c[i];
     }
-    std::vector<State<double>> states(n + 1);
-    std::vector<Hit<double>> hits(n);
-    std::vector<std::array<double, 4>> diracs(n);
-    std::vector<std::array<double, 3>> cols(n);
+    std::vector<State<T>> states(n + 1);
+    std::vector<Hit<T>> hits(n);
+    std::vector<std::array<T, 4>> diracs(n);
+    std::vector<std::array<T, 3>> cols(n);
     states[0] = st;
     for (int i = 0; i < n; ++i) {
-      Hit<double> H;
+      Hit<T> H;
       intersect(&sc.W[9 * ps[i]], &sc.mu[3 * ps[i]], r.o, r.d, H);
       hits[i] = H;
       ts[i] = ex[i] ? H.t1 : H.t0;
-      double c[3];
+      T c[3];
       prim_colour(sc, r, ps[i], c);
-      const double dh = ex[i] ? -sc.sigma[ps[i]] : sc.sigma[ps[i]];
+      const T dh = ex[i] ? -sc.sigma[ps[i]] : sc.sigma[ps[i]];
       diracs[i] = {dh, dh * c[0], dh * c[1], dh * c[2]};
       cols[i] = {c[0], c[1], c[2]};
       states[i + 1] = update(states[i], ts[i], diracs[i].data());
     }
-    const State<double>& fin = states[n];
-    State<double> G;
+    if (inverse_replay) {
+      // the reference's scheme: only the final state is kept; earlier states are undone
+      for (int i = n - 1; i >= 0; --i)
+        states[i] = inverse_update(states[i + 1], diracs[i].data(), i > 0 ? ts[i - 1] : T(0));
+    }
+    const State<T>& fin = states[n];
+    State<T> G;
     const double* go = dout5 + 5 * j;
-    for (int i = 0; i < 3; ++i) G.C[i] = go[i];
-    G.logT = go[3] * std::exp(-fin.logT);  // opacity = 1 - exp(-logT)
-    G.dist[0] = go[4];
-    G.dist[1] = -go[4];
-    double G_o[3] = {0, 0, 0}, G_d[3] = {0, 0, 0}, G_B[16] = {0};
+    for (int i = 0; i < 3; ++i) G.C[i] = T(go[i]);
+    G.logT = T(go[3]) * std::exp(-fin.logT);  // opacity = 1 - exp(-logT)
+    G.dist[0] = T(go[4]);
+    G.dist[1] = -T(go[4]);
+    T G_o[3] = {0, 0, 0}, G_d[3] = {0, 0, 0}, G_B[16] = {0};
     for (int i = n - 1; i >= 0; --i) {
-      State<double> Gs;
-      double Gt, Gdirac[4];
+      State<T> Gs;
+      T Gt, Gdirac[4];
       update_vjp(states[i], ts[i], G, Gs, Gt, Gdirac);
       const int64_t p = ps[i];
-      const double sg = sc.sigma[p];
-      const double sign = ex[i] ? -1.0 : 1.0;
-      const double dh = sign * sg;
+      const T sg = sc.sigma[p];
+      const T sign = ex[i] ? T(-1) : T(1);
+      const T dh = sign * sg;
       // dirac = dh * (1, c)
-      double g_dh = Gdirac[0];
+      T g_dh = Gdirac[0];
       for (int ch = 0; ch < 3; ++ch) g_dh += Gdirac[1 + ch] * cols[i][ch];
       g.sigma[p] += sign * g_dh;
-      const double* f = &sc.feat[(size_t)p * Kc * 3];
+      const T* f = &sc.feat[(size_t)p * Kc * 3];
       for (int ch = 0; ch < 3; ++ch) {
-        const double gc = dh * Gdirac[1 + ch];
+        const T gc = dh * Gdirac[1 + ch];
         for (int k = 0; k < nb; ++k) {
           g.feat[(size_t)p * Kc * 3 + 3 * k + ch] += r.B[k] * gc;
           G_B[k] += f[3 * k + ch] * gc;
         }
       }
       // t from the intersection: |ocn + t rdn|^2 = 1
-      const Hit<double>& H = hits[i];
-      const double t = ts[i];
-      double P[3];
-      for (int a = 0; a < 3; ++a) P[a] = H.ocn[a] + t * H.rdn[a];
-      const double den = P[0] * H.rdn[0] + P[1] * H.rdn[1] + P[2] * H.rdn[2];
-      if (std::fabs(den) > 0.0) {
-        double g_ocn[3], g_rdn[3];
+      const Hit<T>& H = hits[i];
+      const T t = ts[i];
+      // hit point on the unit sphere and d|P|^2/dt / 2, in the cancellation-free form
+      // P = l +- (sqrt(h)/a) rdn, P.rdn = +-sqrt(h) (l: closest point of the line to the centre)
+      T P[3];
+      const T* oc = H.ocn;
+      const T* rn = H.rdn;
+      const T a_ = ffma(rn[2], rn[2], ffma(rn[1], rn[1], rn[0] * rn[0]));
+      const T ba_ = -ffma(oc[2], rn[2], ffma(oc[1], rn[1], oc[0] * rn[0])) / a_;
+      T l_[3];
+      for (int a = 0; a < 3; ++a) l_[a] = ffma(ba_, rn[a], oc[a]);
+      const T ll_ = ffma(l_[2], l_[2], ffma(l_[1], l_[1], l_[0] * l_[0]));
+      const T sh = std::sqrt(fmx(a_ * (T(1) - ll_), T(0)));
+      const T sgn_ = ex[i] ? T(1) : T(-1);
+      for (int a = 0; a < 3; ++a) P[a] = ffma(sgn_ * sh / a_, rn[a], l_[a]);
+      const T den = sgn_ * sh;
+      if (std::fabs(den) > T(K<T>::tiny)) {
+        T g_ocn[3], g_rdn[3];
         for (int a = 0; a < 3; ++a) {
           g_ocn[a] = -Gt * P[a] / den;
           g_rdn[a] = -Gt * t * P[a] / den;
         }
-        const double* Wp = &sc.W[9 * p];
-        const double v[3] = {r.o[0] - sc.mu[3 * p], r.o[1] - sc.mu[3 * p + 1], r.o[2] - sc.mu[3 * p + 2]};
+        const T* Wp = &sc.W[9 * p];
+        const T v[3] = {r.o[0] - sc.mu[3 * p], r.o[1] - sc.mu[3 * p + 1], r.o[2] - sc.mu[3 * p + 2]};
         for (int a = 0; a < 3; ++a)
           for (int b = 0; b < 3; ++b) {
             g.W[9 * p + 3 * a + b] += g_ocn[a] * v[b] + g_rdn[a] * r.d[b];
-            const double wo = Wp[3 * a + b] * g_ocn[a];
+            const T wo = Wp[3 * a + b] * g_ocn[a];
             g.mu[3 * p + b] -= wo;
             G_o[b] += wo;
             G_d[b] += Wp[3 * a + b] * g_rdn[a];
@@ -651,15 +692,15 @@ int backward_impl(int64_t N, int Kc, int deg, const double* mean, const double* 
     }
     // initial density members
     for (int64_t p : members) {
-      double c[3];
+      T c[3];
       prim_colour(sc, r, p, c);
-      const double sg = sc.sigma[p];
-      double g_s = G.drgb[0];
+      const T sg = sc.sigma[p];
+      T g_s = G.drgb[0];
       for (int ch = 0; ch < 3; ++ch) g_s += c[ch] * G.drgb[1 + ch];
       g.sigma[p] += g_s;
-      const double* f = &sc.feat[(size_t)p * Kc * 3];
+      const T* f = &sc.feat[(size_t)p * Kc * 3];
       for (int ch = 0; ch < 3; ++ch) {
-        const double gc = sg * G.drgb[1 + ch];
+        const T gc = sg * G.drgb[1 + ch];
         for (int k = 0; k < nb; ++k) {
           g.feat[(size_t)p * Kc * 3 + 3 * k + ch] += r.B[k] * gc;
           G_B[k] += f[3 * k + ch] * gc;
@@ -667,15 +708,15 @@ int backward_impl(int64_t N, int Kc, int deg, const double* mean, const double* 
       }
     }
     // ray: o = ro + tmin * rd; d = rd / |rd|; SH basis of the raw rd
-    double J[16][3];
+    T J[16][3];
     sh_basis_grad(rd, deg, J);
-    double g_rd[3] = {0, 0, 0};
+    T g_rd[3] = {0, 0, 0};
     for (int k = 0; k < nb; ++k)
       for (int a = 0; a < 3; ++a) g_rd[a] += G_B[k] * J[k][a];
-    const double nrm = std::sqrt(std::fmax(rd[0] * rd[0] + rd[1] * rd[1] + rd[2] * rd[2], K<double>::tiny));
-    const double dG = r.d[0] * G_d[0] + r.d[1] * G_d[1] + r.d[2] * G_d[2];
+    const T nrm = std::sqrt(std::fmax(rd[0] * rd[0] + rd[1] * rd[1] + rd[2] * rd[2], K<T>::tiny));
+    const T dG = r.d[0] * G_d[0] + r.d[1] * G_d[1] + r.d[2] * G_d[2];
     for (int a = 0; a < 3; ++a) {
-      g_rd[a] += (G_d[a] - r.d[a] * dG) / nrm + tmin * G_o[a];
+      g_rd[a] += (G_d[a] - r.d[a] * dG) / nrm + T(tmin) * G_o[a];
       gro[a] = G_o[a];
       grd[a] = g_rd[a];
     }
@@ -692,22 +733,22 @@ int backward_impl(int64_t N, int Kc, int deg, const double* mean, const double* 
   }
   // reduce and convert W gradients to scale / quaternion gradients
   for (int64_t p = 0; p < N; ++p) {
-    double gW[9] = {0}, gmu[3] = {0}, gs = 0;
+    T gW[9] = {0}, gmu[3] = {0}, gs = 0;
     for (auto& g : acc) {
       for (int i = 0; i < 9; ++i) gW[i] += g.W[9 * p + i];
       for (int i = 0; i < 3; ++i) gmu[i] += g.mu[3 * p + i];
       gs += g.sigma[p];
     }
-    const double* q = quat + 4 * p;
-    const double* s = scale + 3 * p;
-    const double* Wp = &sc.W[9 * p];
-    double gscale[3] = {0, 0, 0}, gq[4] = {0, 0, 0, 0};
+    const T q[4] = {T(quat[4 * p]), T(quat[4 * p + 1]), T(quat[4 * p + 2]), T(quat[4 * p + 3])};
+    const T s[3] = {T(scale[3 * p]), T(scale[3 * p + 1]), T(scale[3 * p + 2])};
+    const T* Wp = &sc.W[9 * p];
+    T gscale[3] = {0, 0, 0}, gq[4] = {0, 0, 0, 0};
     for (int i = 0; i < 3; ++i)
       for (int jx = 0; jx < 3; ++jx) gscale[i] -= gW[3 * i + jx] * Wp[3 * i + jx] / s[i];
     for (int jx = 0; jx < 3; ++jx) {
-      double e[3] = {0, 0, 0};
-      e[jx] = 1.0;
-      double gcol[3];
+      T e[3] = {0, 0, 0};
+      e[jx] = T(1);
+      T gcol[3];
       for (int i = 0; i < 3; ++i) gcol[i] = gW[3 * i + jx] / s[i];
       rotate_vector_vjp_q(e, q, gcol, gq);
     }
@@ -718,7 +759,7 @@ int backward_impl(int64_t N, int Kc, int deg, const double* mean, const double* 
     for (int i = 0; i < 4; ++i) out.dquat[4 * p + i] = gq[i];
     out.ddensity[p] = gs;
     for (int i = 0; i < Kc * 3; ++i) {
-      double v = 0;
+      T v = 0;
       for (auto& g : acc) v += g.feat[(size_t)p * Kc * 3 + i];
       out.dfeat[(size_t)p * Kc * 3 + i] = v;
     }
@@ -759,8 +800,33 @@ int ora_backward_f64(int64_t N, int Kc, int deg, const double* mean, const doubl
                      double* dscale, double* dquat, double* ddensity, double* dfeat, double* drayo,
                      double* drayd, int nthreads) {
   BwdOut o{dmean, dscale, dquat, ddensity, dfeat, drayo, drayd};
-  return backward_impl(N, Kc, deg, mean, scale, quat, density, feat, R, rayo, rayd, tmin, tmax, max_iters,
-                       events, iters, dout5, o, nthreads);
+  return backward_impl<double>(N, Kc, deg, mean, scale, quat, density, feat, R, rayo, rayd, tmin, tmax, max_iters,
+                               events, iters, dout5, o, nthreads, false);
+}
+
+// float32 backward with the reference's scheme: the final state is undone event by event
+// (inverse_update_dual) and every VJP runs in float, as the CUDA kernel does. Inputs and
+// outputs are double arrays (values rounded to float inside).
+int ora_backward_f32_stored(int64_t N, int Kc, int deg, const double* mean, const double* scale,
+                            const double* quat, const double* density, const double* feat, int64_t R,
+                            const double* rayo, const double* rayd, double tmin, double tmax, int max_iters,
+                            const int32_t* events, const int32_t* iters, const double* dout5, double* dmean,
+                            double* dscale, double* dquat, double* ddensity, double* dfeat, double* drayo,
+                            double* drayd, int nthreads) {
+  BwdOut o{dmean, dscale, dquat, ddensity, dfeat, drayo, drayd};
+  return backward_impl<float>(N, Kc, deg, mean, scale, quat, density, feat, R, rayo, rayd, tmin, tmax, max_iters,
+                              events, iters, dout5, o, nthreads, false);
+}
+
+int ora_backward_f32_replay(int64_t N, int Kc, int deg, const double* mean, const double* scale,
+                            const double* quat, const double* density, const double* feat, int64_t R,
+                            const double* rayo, const double* rayd, double tmin, double tmax, int max_iters,
+                            const int32_t* events, const int32_t* iters, const double* dout5, double* dmean,
+                            double* dscale, double* dquat, double* ddensity, double* dfeat, double* drayo,
+                            double* drayd, int nthreads) {
+  BwdOut o{dmean, dscale, dquat, ddensity, dfeat, drayo, drayd};
+  return backward_impl<float>(N, Kc, deg, mean, scale, quat, density, feat, R, rayo, rayd, tmin, tmax, max_iters,
+                              events, iters, dout5, o, nthreads, true);
 }
 
 // float32 intersection of one ray with one ellipsoid (for known-answer tests).

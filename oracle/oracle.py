@@ -41,8 +41,12 @@ def lib():
                                     P, P, P, P, P, P, i32]
         L.ora_backward_f64.argtypes = [i64, i32, i32, P, P, P, P, P, i64, P, P, f64, f64, i32,
                                        P, P, P, P, P, P, P, P, P, P, i32]
+        L.ora_backward_f32_replay.argtypes = L.ora_backward_f64.argtypes
+        L.ora_backward_f32_stored.argtypes = L.ora_backward_f64.argtypes
+        L.ora_backward_f32_stored.restype = ctypes.c_int
         L.ora_intersect_f32.argtypes = [P, P, P, P, P, f32, P]
-        for fn in (L.ora_trace_f32, L.ora_trace_f64, L.ora_backward_f64, L.ora_intersect_f32):
+        for fn in (L.ora_trace_f32, L.ora_trace_f64, L.ora_backward_f64, L.ora_backward_f32_replay,
+                   L.ora_intersect_f32):
             fn.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -127,8 +131,14 @@ class Grads:
 
 
 def backward(scene: Scene, rayo, rayd, tmin, tmax, max_iters, events, iters, dout,
-             sh_degree=None, nthreads=None) -> Grads:
-    """FP64 analytic gradients (unclipped) along the given event sequence."""
+             sh_degree=None, nthreads=None, mode="f64") -> Grads:
+    """Gradients (unclipped) along the given event sequence.
+
+    mode "f64": exact FP64 analytic gradients (states stored by a forward replay).
+    mode "f32_replay": the reference's scheme in FP32 (final state undone event by event
+    with inverse_update_dual), which is also what the CUDA backward computes.
+    mode "f32_stored": FP32 with the forward's states stored instead of undone.
+    """
     s = scene.as_dtype(np.float64)
     rayo = np.ascontiguousarray(np.asarray(rayo, np.float64).reshape(-1, 3))
     rayd = np.ascontiguousarray(np.asarray(rayd, np.float64).reshape(-1, 3))
@@ -139,11 +149,13 @@ def backward(scene: Scene, rayo, rayd, tmin, tmax, max_iters, events, iters, dou
     dout = np.ascontiguousarray(np.asarray(dout, np.float64).reshape(R, 5))
     g = Grads(np.zeros((s.N, 3)), np.zeros((s.N, 3)), np.zeros((s.N, 4)), np.zeros(s.N),
               np.zeros((s.N, s.K, 3)), np.zeros((R, 3)), np.zeros((R, 3)))
-    rc = lib().ora_backward_f64(s.N, s.K, deg, _ptr(s.mean), _ptr(s.scale), _ptr(s.quat), _ptr(s.density),
-                                _ptr(s.features), R, _ptr(rayo), _ptr(rayd), float(tmin), float(tmax),
-                                int(max_iters), _ptr(events), _ptr(iters), _ptr(dout), _ptr(g.mean),
-                                _ptr(g.scale), _ptr(g.quat), _ptr(g.density), _ptr(g.features),
-                                _ptr(g.rayo), _ptr(g.rayd), _threads(nthreads))
+    fn = {"f64": lib().ora_backward_f64, "f32_replay": lib().ora_backward_f32_replay,
+          "f32_stored": lib().ora_backward_f32_stored}[mode]
+    rc = fn(s.N, s.K, deg, _ptr(s.mean), _ptr(s.scale), _ptr(s.quat), _ptr(s.density),
+            _ptr(s.features), R, _ptr(rayo), _ptr(rayd), float(tmin), float(tmax),
+            int(max_iters), _ptr(events), _ptr(iters), _ptr(dout), _ptr(g.mean),
+            _ptr(g.scale), _ptr(g.quat), _ptr(g.density), _ptr(g.features),
+            _ptr(g.rayo), _ptr(g.rayd), _threads(nthreads))
     assert rc == 0
     return g
 

@@ -1,0 +1,142 @@
+"""GPU backward parity: gradients of every input tensor against the FP64 analytic
+oracle and against FP64 central differences (the method of the reference's
+tests/grad_check.py), plus the reference's own gradcheck configuration."""
+import numpy as np
+import pytest
+import torch
+
+from ever_b200 import synthetic as S
+from ever_b200.fast_ellipsoid_splinetracer import trace_rays
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+NAMES = ("mean", "scale", "quat", "density", "features")
+
+
+def _dev():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch.device("cuda:0")
+
+
+def _gpu_grads(sc, ro, rd, dout, tmin=0.0, tmax=1000.0, max_iters=500, wcts=None):
+    dev = _dev()
+    t = {k: torch.tensor(np.ascontiguousarray(getattr(sc, k), np.float32), device=dev, requires_grad=True)
+         for k in NAMES}
+    rayo = torch.tensor(np.asarray(ro, np.float32), device=dev, requires_grad=True)
+    rayd = torch.tensor(np.asarray(rd, np.float32), device=dev, requires_grad=True)
+    m2d = torch.zeros((sc.mean.shape[0], 2), device=dev, requires_grad=True) if wcts is not None else None
+    out = trace_rays(t["mean"], t["scale"], t["quat"], t["density"], t["features"], rayo, rayd, tmin, tmax, 3,
+                     m2d, wcts, max_iters)
+    (out * torch.tensor(dout, dtype=torch.float32, device=dev)).sum().backward()
+    g = {k: v.grad.cpu().double().numpy() for k, v in t.items()}
+    g["rayo"] = rayo.grad.cpu().double().numpy()
+    g["rayd"] = rayd.grad.cpu().double().numpy()
+    if m2d is not None:
+        g["means2d"] = m2d.grad.cpu().double().numpy()
+    return g, out.detach().cpu().numpy()
+
+
+def _oracle_grads(sc, ro, rd, dout, tmin=0.0, tmax=1000.0, max_iters=500, mode="f64"):
+    s = O.Scene(sc.mean, sc.scale, sc.quat, np.asarray(sc.density).reshape(-1), sc.features)
+    tr = O.trace(s, ro, rd, tmin, tmax, max_iters)  # float32 event sequence, as the GPU consumed it
+    g = O.backward(s, ro, rd, tmin, tmax, max_iters, tr.events, tr.iters, dout, mode=mode)
+    return {"mean": g.mean, "scale": g.scale, "quat": g.quat, "density": g.density.reshape(-1, 1),
+            "features": g.features, "rayo": g.rayo, "rayd": g.rayd}
+
+
+def _clip(k, v):
+    return np.clip(v, -50, 50) if k == "density" else np.clip(v, -1e3, 1e3)
+
+
+def _rel_err(a, b):
+    return np.abs(a - b).max() / (np.abs(b).max() + 1e-12)
+
+
+# Max abs error relative to the largest gradient entry of that tensor.
+# vs the oracle's FP32 restatement of the same reverse replay (the reference's scheme,
+# backwards_kernel.slang:327-361): differences come only from atomic summation order and
+# the last bits of expf/powf.
+REPLAY_TOL = 1e-4
+# vs exact FP64 gradients: FP32 evaluation of d t / d params ~ 1/sqrt(h) at grazing hits
+# (the largest gradient entries) is conditioned at ~1e-3; the reference's FP32 backward
+# shares this. Measured ~8e-4 on these scenes.
+GRAD_TOL = 5e-3
+
+
+@pytest.mark.parametrize("deg,seed", [(0, 1), (3, 2)])
+def test_gradients_match_fp64_oracle(deg, seed):
+    sc = S.uniform_scene(1500, deg, seed=seed)
+    ro, rd = S.look_at_rays(S.Camera(np.array([0.0, 0.0, 3.0]), 24, 24, 50.0))
+    dout = np.random.default_rng(seed).normal(size=(ro.shape[0], 5))
+    g, _ = _gpu_grads(sc, ro, rd, dout)
+    ref = _oracle_grads(sc, ro, rd, dout)
+    rep = _oracle_grads(sc, ro, rd, dout, mode="f32_replay")
+    for k in ref:
+        assert _rel_err(g[k], _clip(k, rep[k])) < REPLAY_TOL, (k, _rel_err(g[k], _clip(k, rep[k])))
+        assert _rel_err(g[k], _clip(k, ref[k])) < GRAD_TOL, (k, _rel_err(g[k], _clip(k, ref[k])))
+
+
+def test_gradients_rays_inside_and_tmin():
+    sc = S.uniform_scene(1200, 3, seed=5)
+    sc.scale *= 2.5
+    ro, rd = S.look_at_rays(S.Camera(np.array([0.1, 0.0, 0.3]), 16, 16, 80.0))
+    dout = np.random.default_rng(5).normal(size=(ro.shape[0], 5))
+    g, _ = _gpu_grads(sc, ro, rd, dout, tmin=0.05)
+    ref = _oracle_grads(sc, ro, rd, dout, tmin=0.05)
+    rep = _oracle_grads(sc, ro, rd, dout, tmin=0.05, mode="f32_replay")
+    for k in ref:
+        assert _rel_err(g[k], _clip(k, rep[k])) < REPLAY_TOL, (k, _rel_err(g[k], _clip(k, rep[k])))
+        assert _rel_err(g[k], _clip(k, ref[k])) < GRAD_TOL, (k, _rel_err(g[k], _clip(k, ref[k])))
+
+
+@pytest.mark.parametrize("seed", range(4))
+@pytest.mark.parametrize("with_distortion", [False, True])
+def test_reference_gradcheck_configuration(seed, with_distortion):
+    # tests/grad_check.py:134-204: one ellipsoid, quat (0,0,0,1), two rays, random tmin,
+    # loss weights [1,1,1,1,0] or [1,1,1,1,10]; checked against FP64 central differences
+    rng = np.random.default_rng(seed)
+    mean = (2 * rng.random((1, 3)) - 1).astype(np.float32)
+    mean[0, :2] *= 0.2
+    sc = S.SceneArrays(mean, (0.5 * rng.random((1, 3)) + 0.05).astype(np.float32),
+                       np.array([[0, 0, 0, 1.0]], np.float32), (1.1 * rng.random((1, 1)) + 0.05).astype(np.float32),
+                       rng.random((1, 1, 3)).astype(np.float32))
+    ro = np.array([[0, 0, 0], [0, 0, 1.0 if not with_distortion else 0.1]], np.float32)
+    rd = np.array([[0, 0, 1.0], [0, 0, 1.0]], np.float32)
+    tmin = float(rng.random() * 0.3)
+    w = [1, 1, 1, 1, 10] if with_distortion else [1, 1, 1, 1, 0]
+    dout = np.tile(np.asarray(w, np.float64), (2, 1))
+    g, _ = _gpu_grads(sc, ro, rd, dout, tmin=tmin, tmax=100.0)
+    s = O.Scene(sc.mean, sc.scale, sc.quat, sc.density.reshape(-1), sc.features)
+    fd = O.finite_difference(s, ro, rd, tmin, 100.0, 500, dout, eps=1e-6)
+    for k in NAMES + ("rayo", "rayd"):
+        ref = fd[k].reshape(g[k].shape)
+        np.testing.assert_allclose(g[k], _clip(k, ref), atol=1e-2, rtol=1e-2, err_msg=k)
+
+
+def test_means2d_gradient_single_camera():
+    sc = S.uniform_scene(800, 0, seed=13)
+    cam = S.Camera(np.array([0.0, 0.0, 3.0]), 16, 16, 50.0)
+    ro, rd = S.look_at_rays(cam)
+    dout = np.random.default_rng(13).normal(size=(ro.shape[0], 5))
+    wct = torch.eye(4, device=_dev())
+    wct[:3, :3] = torch.tensor([[1.0, 0.2, 0.0], [0.0, 1.0, 0.1], [0.3, 0.0, 1.0]])
+    wct[3, :3] = torch.tensor([0.1, -0.2, 3.0])
+    g, _ = _gpu_grads(sc, ro, rd, dout, wcts=wct.reshape(1, 4, 4))
+    inv = np.linalg.inv(wct.cpu().double().numpy())
+    mean = sc.mean.astype(np.float64)
+    z = mean @ wct.cpu().double().numpy()[:3, 2] + wct[3, 2].item()
+    ref = _oracle_grads(sc, ro, rd, dout, mode="f32_replay")["mean"]
+    expect = z[:, None] * (ref @ inv[:2, :3].T)
+    assert _rel_err(g["means2d"], expect) < REPLAY_TOL
+
+
+def test_truncated_rays_get_no_gradient():
+    # backwards_kernel.slang:304: rays with iters >= max_iters - 1 contribute nothing
+    sc = S.uniform_scene(1500, 0, seed=14)
+    ro, rd = S.look_at_rays(S.Camera(np.array([0.0, 0.0, 3.0]), 8, 8, 30.0))
+    dout = np.ones((ro.shape[0], 5))
+    g, _ = _gpu_grads(sc, ro, rd, dout, max_iters=3)
+    ref = _oracle_grads(sc, ro, rd, dout, max_iters=3, mode="f32_replay")
+    for k in ref:
+        assert _rel_err(g[k], _clip(k, ref[k])) < REPLAY_TOL, k
