@@ -44,6 +44,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--kbuf", type=int, default=0)
     p.add_argument("--block", type=int, default=0)
+    p.add_argument("--verbose", action="store_true", help="per-step device times on stderr")
     return p.parse_args()
 
 
@@ -220,8 +221,16 @@ def main():
                 dist.all_reduce(p.grad)
         return out
 
-    for _ in range(args.warmup):
-        step()
+    for i in range(args.warmup):
+        if args.verbose:
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            step()
+            b.record()
+            torch.cuda.synchronize()
+            print(f"warmup step {i}: {a.elapsed_time(b):.2f} ms", file=sys.stderr, flush=True)
+        else:
+            step()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -229,12 +238,21 @@ def main():
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
         ev0.record()
+        marks = []
         for _ in range(args.steps):
             step()
+            if args.verbose:
+                marks.append(torch.cuda.Event(enable_timing=True))
+                marks[-1].record()
         ev1.record()
         torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
+    if args.verbose:
+        prev = ev0
+        for i, m in enumerate(marks):
+            print(f"timed step {i}: {prev.elapsed_time(m):.2f} ms", file=sys.stderr, flush=True)
+            prev = m
     ms = ev0.elapsed_time(ev1) / args.steps
     ms_t = torch.tensor([ms], device=dev)
     if world > 1:

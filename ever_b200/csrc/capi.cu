@@ -215,13 +215,30 @@ int ever_trace_backward(const EverScene* scene, const float* rayo, const float* 
 }
 
 int ever_event_log_to_reference(const EverScene* scene, const int32_t* event_log, int32_t log_cap,
-                                const int32_t* iters, int64_t num_rays, int32_t* tri_collection, int32_t max_iters,
-                                void* stream) {
+                                const int32_t* iters, int64_t num_rays, const int32_t* ray_order,
+                                int32_t* tri_collection, int32_t max_iters, void* stream) {
   if (!scene || (num_rays > 0 && max_iters > 0 && (!event_log || !iters || !tri_collection)))
     return fail(EVER_ERR_INVALID, "null pointer");
-  return cuda_status(ever::launch_log_to_reference(scene->order, event_log, log_cap, iters, num_rays, tri_collection,
-                                                   max_iters, static_cast<cudaStream_t>(stream)),
+  return cuda_status(ever::launch_log_to_reference(scene->order, event_log, log_cap, iters, num_rays, ray_order,
+                                                   tri_collection, max_iters, static_cast<cudaStream_t>(stream)),
                      "ever_event_log_to_reference");
+}
+
+size_t ever_ray_order_workspace_bytes(int64_t num_rays) {
+  if (num_rays < 0) return 0;
+  return size_t(ever::ray_order_workspace(num_rays));
+}
+
+int ever_ray_order(const float* rayo, const float* rayd, int64_t num_rays, void* workspace, size_t workspace_bytes,
+                   int32_t* ray_order, void* stream) {
+  if (num_rays < 0 || num_rays >= (int64_t(1) << 31)) return fail(EVER_ERR_INVALID, "num_rays out of range");
+  if (num_rays > 0 && (!rayo || !rayd || !ray_order)) return fail(EVER_ERR_INVALID, "null pointer");
+  const int64_t need = ever::ray_order_workspace(num_rays);
+  if (num_rays > 0 && (!workspace || workspace_bytes < size_t(need)))
+    return fail(EVER_ERR_WORKSPACE, "ray order workspace needs %lld bytes, got %zu", (long long)need, workspace_bytes);
+  return cuda_status(ever::ray_order(rayo, rayd, num_rays, static_cast<char*>(workspace), ray_order,
+                                     static_cast<cudaStream_t>(stream)),
+                     "ever_ray_order");
 }
 
 }  // extern "C"

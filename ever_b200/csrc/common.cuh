@@ -162,7 +162,7 @@ __host__ __device__ __forceinline__ int feat_stride(int K) { return (3 * K + 3) 
 // Colour of an ellipsoid along the ray: sum_k B_k f_k + 0.5 (eval_color, sh.slang:90-103).
 // f: the ellipsoid's 16-byte aligned feature row.
 template <int DEG>
-__device__ __forceinline__ float3 sh_colour(const float* __restrict__ f, const float* B) {
+__device__ __forceinline__ float3 sh_colour(const float* __restrict__ f, const float* B, int bs = 1) {
   constexpr int NB = (DEG + 1) * (DEG + 1);
   constexpr int NV = (3 * NB + 3) / 4;
   float v[4 * NV];
@@ -175,12 +175,14 @@ __device__ __forceinline__ float3 sh_colour(const float* __restrict__ f, const f
     v[4 * i + 2] = x.z;
     v[4 * i + 3] = x.w;
   }
-  float3 c = make_float3(fmaf(B[0], v[0], 0.5f), fmaf(B[0], v[1], 0.5f), fmaf(B[0], v[2], 0.5f));
+  const float b0 = B[0];
+  float3 c = make_float3(fmaf(b0, v[0], 0.5f), fmaf(b0, v[1], 0.5f), fmaf(b0, v[2], 0.5f));
 #pragma unroll
   for (int k = 1; k < NB; ++k) {
-    c.x = fmaf(B[k], v[3 * k + 0], c.x);
-    c.y = fmaf(B[k], v[3 * k + 1], c.y);
-    c.z = fmaf(B[k], v[3 * k + 2], c.z);
+    const float bk = B[k * bs];
+    c.x = fmaf(bk, v[3 * k + 0], c.x);
+    c.y = fmaf(bk, v[3 * k + 1], c.y);
+    c.z = fmaf(bk, v[3 * k + 2], c.z);
   }
   return c;
 }

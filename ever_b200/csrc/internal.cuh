@@ -28,6 +28,11 @@ struct SceneLayout {
 };
 
 SceneLayout scene_layout(int64_t N, int K);
+int sort_blocks(int64_t N);
+void sort_pairs(uint32_t*& ka, uint32_t*& va, uint32_t*& kb, uint32_t*& vb, uint32_t* hist, int64_t N, int bits,
+                cudaStream_t st);
+int64_t ray_order_workspace(int64_t R);
+cudaError_t ray_order(const float* rayo, const float* rayd, int64_t R, char* ws, int32_t* order, cudaStream_t st);
 cudaError_t scene_build(const float* mean, const float* scale, const float* quat, const float* density,
                         const float* feat, int64_t N, int K, char* ws, const SceneLayout& L, EverScene* sc,
                         cudaStream_t st);
@@ -97,6 +102,6 @@ struct FinalizeParams {
 
 cudaError_t launch_finalize(const FinalizeParams& P, cudaStream_t st);
 cudaError_t launch_log_to_reference(const int32_t* order, const int32_t* log, int log_cap, const int32_t* iters,
-                                    int64_t R, int32_t* tri, int max_iters, cudaStream_t st);
+                                    int64_t R, const int32_t* ray_order, int32_t* tri, int max_iters, cudaStream_t st);
 
 }  // namespace ever

@@ -1,0 +1,76 @@
+// Coherent ray order for the packet traversal: rays are sorted by a 32-bit key made of
+// a coarse origin cell (6 bits) above the Morton code of the octahedral projection of
+// the direction (12 bits per axis). Thirty-two consecutive rays of the result then cover
+// a compact patch of directions (a screen tile for a pinhole camera), so a warp's packet
+// walks far fewer nodes than a scanline strip would. The order only decides which
+// thread picks up which ray; results do not depend on it.
+#include "common.cuh"
+#include "internal.cuh"
+
+namespace ever {
+namespace {
+
+__device__ __forceinline__ uint32_t spread2(uint32_t v) {  // 16 bits -> even bits
+  v &= 0xffffu;
+  v = (v | (v << 8)) & 0x00ff00ffu;
+  v = (v | (v << 4)) & 0x0f0f0f0fu;
+  v = (v | (v << 2)) & 0x33333333u;
+  v = (v | (v << 1)) & 0x55555555u;
+  return v;
+}
+
+__global__ void k_ray_keys(const float* __restrict__ rayo, const float* __restrict__ rayd, int64_t R,
+                           uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  const int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  float dx = rayd[3 * r], dy = rayd[3 * r + 1], dz = rayd[3 * r + 2];
+  const float l1 = fabsf(dx) + fabsf(dy) + fabsf(dz);
+  float u = 0.f, v = 0.f;
+  if (l1 > 0.f && isfinite(l1)) {
+    u = dx / l1;
+    v = dy / l1;
+    if (dz < 0.f) {
+      const float uu = (1.f - fabsf(v)) * (u >= 0.f ? 1.f : -1.f);
+      const float vv = (1.f - fabsf(u)) * (v >= 0.f ? 1.f : -1.f);
+      u = uu;
+      v = vv;
+    }
+  }
+  const uint32_t qu = min(uint32_t(fmaxf(u * 0.5f + 0.5f, 0.f) * 4096.f), 4095u);
+  const uint32_t qv = min(uint32_t(fmaxf(v * 0.5f + 0.5f, 0.f) * 4096.f), 4095u);
+  uint32_t cell = 0;
+  for (int a = 0; a < 3; ++a) {
+    const float o = rayo[3 * r + a];
+    const uint32_t q = o == o ? uint32_t(fminf(fmaxf((o + 4.f) * 0.5f, 0.f), 3.f)) : 0u;  // 4 cells on [-4, 4]
+    cell = (cell << 2) | q;
+  }
+  keys[r] = (cell << 24) | (spread2(qu) << 1) | spread2(qv);
+  vals[r] = uint32_t(r);
+}
+
+}  // namespace
+
+int64_t ray_order_workspace(int64_t R) {
+  WsCursor c;
+  c.take(R * 4);
+  c.take(R * 4);
+  c.take(R * 4);
+  c.take(R * 4);
+  c.take(int64_t(sort_blocks(R)) * 256 * 4);
+  return c.offset;
+}
+
+cudaError_t ray_order(const float* rayo, const float* rayd, int64_t R, char* ws, int32_t* order, cudaStream_t st) {
+  if (R == 0) return cudaSuccess;
+  WsCursor c;
+  uint32_t* ka = reinterpret_cast<uint32_t*>(ws + c.take(R * 4));
+  uint32_t* va = reinterpret_cast<uint32_t*>(ws + c.take(R * 4));
+  uint32_t* kb = reinterpret_cast<uint32_t*>(ws + c.take(R * 4));
+  uint32_t* vb = reinterpret_cast<uint32_t*>(ws + c.take(R * 4));
+  uint32_t* hist = reinterpret_cast<uint32_t*>(ws + c.take(int64_t(sort_blocks(R)) * 256 * 4));
+  k_ray_keys<<<unsigned((R + 255) / 256), 256, 0, st>>>(rayo, rayd, R, ka, va);
+  sort_pairs(ka, va, kb, vb, hist, R, 30, st);
+  return cudaMemcpyAsync(order, va, R * sizeof(int32_t), cudaMemcpyDeviceToDevice, st);
+}
+
+}  // namespace ever

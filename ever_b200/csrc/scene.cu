@@ -365,6 +365,23 @@ inline int64_t div_up(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
 }  // namespace
 
+int sort_blocks(int64_t N) { return int(div_up(std::max<int64_t>(N, 1), kSortTile)); }
+
+// Stable LSD radix sort of (key, value) pairs on the low `bits` key bits, 8 bits per pass.
+// On return the sorted pairs are in (ka, va); (kb, vb) are scratch of the same size and
+// hist holds sort_blocks(N) * 256 words.
+void sort_pairs(uint32_t*& ka, uint32_t*& va, uint32_t*& kb, uint32_t*& vb, uint32_t* hist, int64_t N, int bits,
+                cudaStream_t st) {
+  const int nblocks = sort_blocks(N);
+  for (int shift = 0; shift < bits; shift += 8) {
+    k_sort_hist<<<nblocks, kSortThreads, 0, st>>>(ka, N, shift, hist, nblocks);
+    k_sort_scan<<<1, 1024, 0, st>>>(hist, int64_t(nblocks) * 256);
+    k_sort_scatter<<<nblocks, kSortThreads, 0, st>>>(ka, va, kb, vb, N, shift, hist, nblocks);
+    std::swap(ka, kb);
+    std::swap(va, vb);
+  }
+}
+
 SceneLayout scene_layout(int64_t N, int K) {
   SceneLayout L;
   WsCursor c;
@@ -379,7 +396,7 @@ SceneLayout scene_layout(int64_t N, int K) {
   L.keys_b = c.take(N * sizeof(uint32_t));
   L.vals_a = c.take(N * sizeof(uint32_t));
   L.vals_b = c.take(N * sizeof(uint32_t));
-  L.nblocks = int(div_up(std::max<int64_t>(N, 1), kSortTile));
+  L.nblocks = sort_blocks(N);
   L.hist = c.take(int64_t(L.nblocks) * 256 * sizeof(uint32_t));
   L.parent_node = c.take(std::max<int64_t>(n1, 1) * sizeof(int32_t));
   L.parent_leaf = c.take(std::max<int64_t>(N, 1) * sizeof(int32_t));
@@ -422,14 +439,7 @@ cudaError_t scene_build(const float* mean, const float* scale, const float* quat
   k_aabbs<<<unsigned(gb), tb, 0, st>>>(mean, scale, quat, N, aabb_a, bounds);
   k_morton<<<unsigned(gb), tb, 0, st>>>(aabb_a, N, bounds, ka, va);
   // 30-bit keys: 4 passes of 8 bits
-  for (int pass = 0; pass < 4; ++pass) {
-    const int shift = 8 * pass;
-    k_sort_hist<<<L.nblocks, kSortThreads, 0, st>>>(ka, N, shift, hist, L.nblocks);
-    k_sort_scan<<<1, 1024, 0, st>>>(hist, int64_t(L.nblocks) * 256);
-    k_sort_scatter<<<L.nblocks, kSortThreads, 0, st>>>(ka, va, kb, vb, N, shift, hist, L.nblocks);
-    std::swap(ka, kb);
-    std::swap(va, vb);
-  }
+  sort_pairs(ka, va, kb, vb, hist, N, 30, st);
   k_gather<<<unsigned(gb), tb, 0, st>>>(va, N, K, mean, scale, quat, density, feat, aabb_a, aabb_b,
                                         reinterpret_cast<Record*>(sc->records), sc->features, sc->order);
   if (N == 1) {

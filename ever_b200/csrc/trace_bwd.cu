@@ -271,7 +271,6 @@ __global__ void __launch_bounds__(256) k_trace_bwd(const BwdParams P) {
     grd[0] = grd[1] = grd[2] = 0.f;
     return;
   }
-  constexpr int NB = (DEG + 1) * (DEG + 1);
   const Node* nodes = reinterpret_cast<const Node*>(P.nodes);
   const Record* recs = reinterpret_cast<const Record*>(P.records);
   const float3 ro = make_float3(P.rayo[3 * r], P.rayo[3 * r + 1], P.rayo[3 * r + 2]);
@@ -318,11 +317,11 @@ __global__ void __launch_bounds__(256) k_trace_bwd(const BwdParams P) {
 #pragma unroll
   for (int k = 0; k < 16; ++k) GB[k] = 0.f;
 
-  Ctrl cur = load_ctrl<DEG>(recs, P.features, fstride, ray, B, P.event_log[int64_t(n - 1) * P.R + r]);
+  Ctrl cur = load_ctrl<DEG>(recs, P.features, fstride, ray, B, P.event_log[int64_t(n - 1) * P.R + gi]);
   for (int i = n - 1; i >= 0; --i) {
     Ctrl old;
     if (i > 0) {
-      old = load_ctrl<DEG>(recs, P.features, fstride, ray, B, P.event_log[int64_t(i - 1) * P.R + r]);
+      old = load_ctrl<DEG>(recs, P.features, fstride, ray, B, P.event_log[int64_t(i - 1) * P.R + gi]);
     } else {
       old.t = 0.f;
       old.dirac = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -520,18 +519,20 @@ __global__ void k_finalize(const FinalizeParams P) {
   }
 }
 
+// tri[i * R + ray] from log[i * R + slot], ray = ray_order[slot] (or slot).
 __global__ void k_log_to_reference(const int32_t* __restrict__ order, const int32_t* __restrict__ log, int log_cap,
-                                   const int32_t* __restrict__ iters, int64_t R, int32_t* __restrict__ tri,
-                                   int max_iters) {
+                                   const int32_t* __restrict__ iters, int64_t R, const int32_t* __restrict__ ray_order,
+                                   int32_t* __restrict__ tri, int max_iters) {
   const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= R * int64_t(max_iters)) return;
-  const int64_t i = t / R, r = t - i * R;
+  const int64_t i = t / R, slot = t - i * R;
+  const int64_t r = ray_order ? int64_t(ray_order[slot]) : slot;
   int32_t v = 0;
   if (i < iters[r] && i < log_cap) {
-    const int32_t id = log[i * R + r];
+    const int32_t id = log[i * R + slot];
     v = 2 * order[id >> 1] + (id & 1);
   }
-  tri[t] = v;
+  tri[i * R + r] = v;
 }
 
 template <int DEG>
@@ -564,10 +565,11 @@ cudaError_t launch_finalize(const FinalizeParams& P, cudaStream_t st) {
 }
 
 cudaError_t launch_log_to_reference(const int32_t* order, const int32_t* log, int log_cap, const int32_t* iters,
-                                    int64_t R, int32_t* tri, int max_iters, cudaStream_t st) {
+                                    int64_t R, const int32_t* ray_order, int32_t* tri, int max_iters, cudaStream_t st) {
   const int64_t total = R * int64_t(max_iters);
   if (total == 0) return cudaSuccess;
-  k_log_to_reference<<<unsigned((total + 255) / 256), 256, 0, st>>>(order, log, log_cap, iters, R, tri, max_iters);
+  k_log_to_reference<<<unsigned((total + 255) / 256), 256, 0, st>>>(order, log, log_cap, iters, R, ray_order, tri,
+                                                                    max_iters);
   return cudaGetLastError();
 }
 

@@ -169,7 +169,11 @@ __device__ void gather_packet(const Node* __restrict__ nodes, const Record* __re
       const unsigned pref0 = __ballot_sync(kFull, t0 <= t1 && t0 != INFINITY);
       const bool first0 = 2 * __popc(pref0) >= __popc(m0 | m1);
       if (sp < kStackDepth) {
-        if (lane == 0) wstack[sp] = first0 ? c1 : c0;
+        if (lane == 0) {
+          const int far = first0 ? c1 : c0;
+          wstack[sp] = far;
+          asm volatile("prefetch.global.L1 [%0];" ::"l"(nodes + far));
+        }
         ++sp;
       } else {
         status |= EVER_STATUS_STACK_OVERFLOW;
@@ -207,7 +211,7 @@ __device__ __forceinline__ void member_insert(int p, int j, int& n_mem, int (&me
 // beyond kMaxMembers the rest are summed into `extra` in traversal order (status flag).
 template <int DEG>
 __device__ __forceinline__ void point_leaf(const Record* __restrict__ recs, const float* __restrict__ feats, int fst,
-                                           const float* B, const Ray& ray, int j, int& n_mem,
+                                           const float* B, int bs, const Ray& ray, int j, int& n_mem,
                                            int (&mem_p)[kMaxMembers], int (&mem_j)[kMaxMembers], float4& extra,
                                            uint32_t& status) {
   const Record R = load_record(recs, j);
@@ -218,7 +222,7 @@ __device__ __forceinline__ void point_leaf(const Record* __restrict__ recs, cons
   } else {
     status |= EVER_STATUS_INIT_OVERFLOW;
     const float sg = R.r3.x;
-    const float3 c = sh_colour<DEG>(feats + int64_t(j) * fst, B);
+    const float3 c = sh_colour<DEG>(feats + int64_t(j) * fst, B, bs);
     extra.x = extra.x + sg;
     extra.y = extra.y + sg * c.x;
     extra.z = extra.z + sg * c.y;
@@ -229,7 +233,7 @@ __device__ __forceinline__ void point_leaf(const Record* __restrict__ recs, cons
 // Point query for the ray start; PACKET: warp-uniform walk.
 template <int DEG, bool PACKET>
 __device__ int point_members(const Node* __restrict__ nodes, const Record* __restrict__ recs,
-                             const float* __restrict__ feats, int fst, const float* B, const Ray& ray, bool act,
+                             const float* __restrict__ feats, int fst, const float* B, int bs, const Ray& ray, bool act,
                              int* stack, int stride, int lane, int (&mem_p)[kMaxMembers], int (&mem_j)[kMaxMembers],
                              float4& extra, uint32_t& status) {
   int n_mem = 0;
@@ -240,8 +244,8 @@ __device__ int point_members(const Node* __restrict__ nodes, const Record* __res
     const bool h0 = act && box_contains(nd.a.x, nd.a.y, nd.a.z, nd.a.w, nd.b.x, nd.b.y, ray.o);
     const bool h1 = act && box_contains(nd.b.z, nd.b.w, nd.c.x, nd.c.y, nd.c.z, nd.c.w, ray.o);
     const int c0 = nd.d.x, c1 = nd.d.y;
-    if (h0 && c0 < 0) point_leaf<DEG>(recs, feats, fst, B, ray, ~c0, n_mem, mem_p, mem_j, extra, status);
-    if (h1 && c1 < 0) point_leaf<DEG>(recs, feats, fst, B, ray, ~c1, n_mem, mem_p, mem_j, extra, status);
+    if (h0 && c0 < 0) point_leaf<DEG>(recs, feats, fst, B, bs, ray, ~c0, n_mem, mem_p, mem_j, extra, status);
+    if (h1 && c1 < 0) point_leaf<DEG>(recs, feats, fst, B, bs, ray, ~c1, n_mem, mem_p, mem_j, extra, status);
     bool g0 = h0 && c0 >= 0, g1 = h1 && c1 >= 0;
     if (PACKET) {
       g0 = __any_sync(kFull, g0);
@@ -270,7 +274,7 @@ __device__ int point_members(const Node* __restrict__ nodes, const Record* __res
 // Integrates the gathered events in order. Returns true once the ray is finished.
 template <int KBUF, int DEG>
 __device__ __forceinline__ bool consume(const FwdParams& P, const Record* __restrict__ recs, const Ray& ray,
-                                        const float* B, int64_t r, uint64_t (&buf)[KBUF], State& s,
+                                        const float* B, int bs, int64_t slot, uint64_t (&buf)[KBUF], State& s,
                                         float4& last_dirac, int& iters, float& s16, int& cnt16, uint64_t& lower,
                                         uint32_t& status) {
   const int fst = feat_stride(P.K);
@@ -293,14 +297,14 @@ __device__ __forceinline__ bool consume(const FwdParams& P, const Record* __rest
       intersect(load_record(recs, j), ray, H);
       if (!(H.t0 > s16 && H.t0 <= P.tmax)) continue;
     }
-    const float3 c = sh_colour<DEG>(P.features + int64_t(j) * fst, B);
+    const float3 c = sh_colour<DEG>(P.features + int64_t(j) * fst, B, bs);
     const float dh = ex ? -r3.x : r3.x;
     const float4 dirac = make_float4(dh, dh * c.x, dh * c.y, dh * c.z);
     update(s, t, dirac);
     last_dirac = dirac;
     if (P.out.event_log) {
       if (iters < P.out.log_cap)
-        P.out.event_log[int64_t(iters) * P.R + r] = 2 * j + (ex ? 0 : 1);
+        P.out.event_log[int64_t(iters) * P.R + slot] = 2 * j + (ex ? 0 : 1);
       else
         status |= EVER_STATUS_LOG_OVERFLOW;
     }
@@ -318,14 +322,14 @@ __device__ __forceinline__ bool consume(const FwdParams& P, const Record* __rest
 }
 
 template <int DEG>
-__device__ __forceinline__ void init_density(const FwdParams& P, const Record* recs, const float* B, int n_mem,
+__device__ __forceinline__ void init_density(const FwdParams& P, const Record* recs, const float* B, int bs, int n_mem,
                                              const int (&mem_j)[kMaxMembers], float4 extra, uint32_t status,
                                              State& s) {
   const int fst = feat_stride(P.K);
   for (int q = 0; q < n_mem; ++q) {
     const int j = mem_j[q];
     const float sg = __ldg(&recs[j].r3.x);
-    const float3 c = sh_colour<DEG>(P.features + int64_t(j) * fst, B);
+    const float3 c = sh_colour<DEG>(P.features + int64_t(j) * fst, B, bs);
     s.drgb.x = s.drgb.x + sg;
     s.drgb.y = s.drgb.y + sg * c.x;
     s.drgb.z = s.drgb.z + sg * c.y;
@@ -391,9 +395,9 @@ __global__ void __launch_bounds__(256) k_trace_fwd_ray(const FwdParams P) {
   if (P.N > 0) {
     int mem_p[kMaxMembers], mem_j[kMaxMembers];
     float4 extra = make_float4(0.f, 0.f, 0.f, 0.f);
-    const int n_mem = point_members<DEG, false>(nodes, recs, P.features, feat_stride(P.K), B, ray, true, st_node,
+    const int n_mem = point_members<DEG, false>(nodes, recs, P.features, feat_stride(P.K), B, 1, ray, true, st_node,
                                                 stride, 0, mem_p, mem_j, extra, status);
-    init_density<DEG>(P, recs, B, n_mem, mem_j, extra, status, s);
+    init_density<DEG>(P, recs, B, 1, n_mem, mem_j, extra, status, s);
     float s16 = 0.f;
     int cnt16 = 0;
     uint64_t lower = 0;
@@ -403,7 +407,7 @@ __global__ void __launch_bounds__(256) k_trace_fwd_ray(const FwdParams P) {
 #pragma unroll
       for (int i = 0; i < KBUF; ++i) buf[i] = kEmptyKey;
       gather_ray<KBUF>(nodes, recs, ray, sl, lower, s16, P.tmax, buf, st_node, st_t, stride, status);
-      done = consume<KBUF, DEG>(P, recs, ray, B, r, buf, s, last_dirac, iters, s16, cnt16, lower, status);
+      done = consume<KBUF, DEG>(P, recs, ray, B, 1, gi, buf, s, last_dirac, iters, s16, cnt16, lower, status);
     }
   }
   write_outputs(P, r, s, last_dirac, iters, status);
@@ -414,6 +418,8 @@ __global__ void __launch_bounds__(256) k_trace_fwd_packet(const FwdParams P) {
   extern __shared__ int smem[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   int* wstack = smem + warp * kStackDepth;
+  float* B = reinterpret_cast<float*>(smem + (blockDim.x / 32) * kStackDepth) + tid;  // B[k * blockDim.x]
+  const int bs = blockDim.x;
   const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;
   const bool valid = gi < P.R;  // every lane stays for the warp-wide ballots
   const int64_t r = valid ? (P.ray_order ? int64_t(P.ray_order[gi]) : gi) : 0;
@@ -421,8 +427,12 @@ __global__ void __launch_bounds__(256) k_trace_fwd_packet(const FwdParams P) {
   const Record* recs = reinterpret_cast<const Record*>(P.records);
   const Ray ray = load_ray(P, r);
   const RaySlab sl = make_slab(ray);
-  float B[16];
-  sh_basis<DEG>(ray.rd, B);
+  {
+    float Bl[16];
+    sh_basis<DEG>(ray.rd, Bl);
+#pragma unroll
+    for (int k = 0; k < (DEG + 1) * (DEG + 1); ++k) B[k * bs] = Bl[k];
+  }
   uint32_t status = 0;
   State s = empty_state();
   float4 last_dirac = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -430,9 +440,9 @@ __global__ void __launch_bounds__(256) k_trace_fwd_packet(const FwdParams P) {
   if (P.N > 0) {
     int mem_p[kMaxMembers], mem_j[kMaxMembers];
     float4 extra = make_float4(0.f, 0.f, 0.f, 0.f);
-    const int n_mem = point_members<DEG, true>(nodes, recs, P.features, feat_stride(P.K), B, ray, valid, wstack, 1,
-                                               lane, mem_p, mem_j, extra, status);
-    init_density<DEG>(P, recs, B, n_mem, mem_j, extra, status, s);
+    const int n_mem = point_members<DEG, true>(nodes, recs, P.features, feat_stride(P.K), B, bs, ray, valid, wstack,
+                                               1, lane, mem_p, mem_j, extra, status);
+    init_density<DEG>(P, recs, B, bs, n_mem, mem_j, extra, status, s);
     float s16 = 0.f;
     int cnt16 = 0;
     uint64_t lower = 0;
@@ -442,7 +452,7 @@ __global__ void __launch_bounds__(256) k_trace_fwd_packet(const FwdParams P) {
 #pragma unroll
       for (int i = 0; i < KBUF; ++i) buf[i] = kEmptyKey;
       gather_packet<KBUF>(nodes, recs, ray, sl, act, lower, s16, P.tmax, buf, wstack, lane, status);
-      if (act) act = !consume<KBUF, DEG>(P, recs, ray, B, r, buf, s, last_dirac, iters, s16, cnt16, lower, status);
+      if (act) act = !consume<KBUF, DEG>(P, recs, ray, B, bs, gi, buf, s, last_dirac, iters, s16, cnt16, lower, status);
     }
   }
   if (valid) write_outputs(P, r, s, last_dirac, iters, status);
@@ -458,7 +468,7 @@ cudaError_t launch_t(const FwdParams& P, int block, int traversal, cudaStream_t 
     if (e != cudaSuccess) return e;
     kern<<<unsigned(grid), block, smem, st>>>(P);
   } else {
-    const size_t smem = size_t(kStackDepth) * (block / 32) * sizeof(int);
+    const size_t smem = size_t(kStackDepth) * (block / 32) * sizeof(int) + size_t(16) * block * sizeof(float);
     k_trace_fwd_packet<KBUF, DEG><<<unsigned(grid), block, smem, st>>>(P);
   }
   return cudaGetLastError();

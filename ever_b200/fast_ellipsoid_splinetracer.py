@@ -19,6 +19,11 @@ colour of each ellipsoid is evaluated along the ray direction rayd, as the refer
 backward evaluates it (backwards_kernel.slang:162, 238). At degree 0 (the trainer's
 case) this equals the reference's forward, which reads only the DC term; pass
 sh_degree=0 to get that DC-only colour with higher-degree features too.
+
+Launch order: by default the rays are first sorted into a coherent order on the device
+(ray_order="auto", see ever_ray_order in include/ever_b200.h) so that each warp's packet
+covers a compact patch of directions; pass ray_order=None for the given order or an
+int32 permutation of your own. Results never depend on it.
 """
 from __future__ import annotations
 
@@ -63,12 +68,19 @@ class SplineTracer(Function):
         return_extras: bool = False,
         sh_degree: int | None = None,
         tune: T.Tune | None = None,
+        ray_order="auto",
     ):
         ctx.device = rayo.device
         scene = T.Scene(mean, scale, quat, density, color)
         needs_grad = any(ctx.needs_input_grad[:7]) or (mean2D is not None and ctx.needs_input_grad[10])
+        if isinstance(ray_order, str):
+            if ray_order != "auto":
+                raise RuntimeError(f"ray_order must be 'auto', None or an int32 tensor, got {ray_order!r}")
+            ray_order = T.ray_order(rayo, rayd) if rayo.shape[0] > 0 else None
         fwd = T.forward(scene, rayo, rayd, tmin, tmax, max_iters, sh_degree,
-                        log_events=needs_grad or return_extras, touch_count=return_extras, tune=tune)
+                        log_events=needs_grad or return_extras, touch_count=return_extras, ray_order=ray_order,
+                        tune=tune)
+        ctx.ray_order = ray_order
         ctx.scene = scene
         ctx.fwd = fwd
         ctx.tmin, ctx.tmax, ctx.max_iters = tmin, tmax, max_iters
@@ -82,7 +94,8 @@ class SplineTracer(Function):
         if return_extras:
             saved = SavedForBackward(fwd.states, fwd.last_dirac, fwd.iters, fwd.touch_count)
             return out, dict(
-                tri_collection=T.reference_tri_collection(scene, fwd, max_iters) if fwd.event_log is not None
+                tri_collection=T.reference_tri_collection(scene, fwd, max_iters, ray_order)
+                if fwd.event_log is not None
                 else torch.zeros(rayo.shape[0] * max_iters, dtype=torch.int32, device=rayo.device),
                 iters=fwd.iters,
                 opacity=out[:, 3],
@@ -96,7 +109,10 @@ class SplineTracer(Function):
     def backward(ctx, grad_output: torch.Tensor, *unused):
         rayo, rayd, wcts = ctx.saved_tensors
         g = T.backward(ctx.scene, rayo, rayd, ctx.fwd, grad_output, ctx.tmin, ctx.tmax, ctx.max_iters,
-                       ctx.sh_degree, wcts=wcts, want_means2d=ctx.has_wcts, tune=ctx.tune)
+                       ctx.sh_degree, wcts=wcts, want_means2d=ctx.has_wcts, ray_order=ctx.ray_order, tune=ctx.tune)
+        # the event log and scene workspace are not needed again: give them back to the allocator
+        ctx.fwd = None
+        ctx.scene = None
         return (
             g.mean,
             g.scale,
@@ -109,6 +125,7 @@ class SplineTracer(Function):
             None,
             None,
             g.means2d,
+            None,
             None,
             None,
             None,
@@ -134,9 +151,10 @@ def trace_rays(
     return_extras: bool = False,
     sh_degree: int | None = None,
     tune: T.Tune | None = None,
+    ray_order="auto",
 ):
     return SplineTracer.apply(mean, scale, quat, density, features, rayo, rayd, tmin, tmax, max_prim_size,
-                              dL_dmeans2D, wcts, max_iters, return_extras, sh_degree, tune)
+                              dL_dmeans2D, wcts, max_iters, return_extras, sh_degree, tune, ray_order)
 
 
 trace_rays.uses_density = True

@@ -198,7 +198,26 @@ def backward(scene: Scene, rayo, rayd, fwd: ForwardResult, grad_out, tmin=0.0, t
     return g
 
 
-def reference_tri_collection(scene: Scene, fwd: ForwardResult, max_iters: int) -> torch.Tensor:
+def ray_order(rayo, rayd, workspace: torch.Tensor | None = None) -> torch.Tensor:
+    """A coherent launch order (int32 permutation) for the packet traversal."""
+    device = rayo.device
+    _check_tensor("ray_origins", rayo, device, 3)
+    _check_tensor("ray_directions", rayd, device, 3)
+    rayo = rayo.contiguous()
+    rayd = rayd.contiguous()
+    R = rayo.numel() // 3
+    order = torch.empty(R, dtype=torch.int32, device=device)
+    lib = N.load()
+    need = int(lib.ever_ray_order_workspace_bytes(R))
+    if workspace is None or workspace.numel() < need:
+        workspace = torch.empty(max(need, 256), dtype=torch.uint8, device=device)
+    with torch.cuda.device(device):
+        N.check(lib.ever_ray_order(N.ptr(rayo), N.ptr(rayd), R, N.ptr(workspace), int(workspace.numel()),
+                                   N.ptr(order), _stream(device)))
+    return order
+
+
+def reference_tri_collection(scene: Scene, fwd: ForwardResult, max_iters: int, ray_order=None) -> torch.Tensor:
     """The reference's tri_collection: (R*max_iters,) int32, iteration-major, original ids."""
     R = fwd.iters.numel()
     log = fwd.event_log
@@ -208,5 +227,6 @@ def reference_tri_collection(scene: Scene, fwd: ForwardResult, max_iters: int) -
     with torch.cuda.device(scene.device):
         N.check(N.load().ever_event_log_to_reference(ctypes.byref(scene.c), N.ptr(log),
                                                      0 if log is None else log.shape[0], N.ptr(fwd.iters), R,
-                                                     N.ptr(tri), int(max_iters), _stream(scene.device)))
+                                                     N.ptr(ray_order), N.ptr(tri), int(max_iters),
+                                                     _stream(scene.device)))
     return tri

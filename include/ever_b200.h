@@ -65,7 +65,8 @@ typedef struct EverForwardOut {
   float* last_dirac;   /* (R,4) dirac of the last consumed event */
   int32_t* iters;      /* (R) consumed events (required) */
   int32_t* event_log;  /* (log_cap, R) iteration-major event ids in Morton numbering
-                          (2j+1 entry, 2j exit); needed by backward */
+                          (2j+1 entry, 2j exit); column = launch slot (ray ray_order[slot],
+                          or ray slot without ray_order); needed by backward */
   int32_t log_cap;     /* rows of event_log (>= max_iters to log every event) */
   int32_t* touch_count;/* (N) original order: events per ellipsoid (atomic, exact) */
   float* ray_stats;    /* (R,2): consumed events, termination depth (t of last event) */
@@ -140,11 +141,22 @@ int ever_trace_backward(const EverScene* scene, const float* rayo, const float* 
                         void* stream);
 
 /* Converts an event log in Morton numbering into the reference's tri_collection ids
- * (2p+1 entry, 2p exit with original indices p; fast_ellipsoid_splinetracer.py:93-101).
+ * (2p+1 entry, 2p exit with original indices p; fast_ellipsoid_splinetracer.py:93-101),
+ * (max_iters, R) indexed by ray. ray_order: the order the forward was launched with.
  * Entries at or beyond iters[r] are set to 0, as the reference's zero-filled buffer. */
 int ever_event_log_to_reference(const EverScene* scene, const int32_t* event_log, int32_t log_cap,
-                                const int32_t* iters, int64_t num_rays, int32_t* tri_collection,
-                                int32_t max_iters, void* stream);
+                                const int32_t* iters, int64_t num_rays, const int32_t* ray_order,
+                                int32_t* tri_collection, int32_t max_iters, void* stream);
+
+/* Bytes of workspace ever_ray_order() needs for R rays. */
+size_t ever_ray_order_workspace_bytes(int64_t num_rays);
+
+/* A coherent launch order for R rays (no counterpart in the reference, whose OptiX
+ * launch order is the ray index): rays sorted by a coarse origin cell and the Morton
+ * code of their octahedral direction, so each warp's packet covers a compact patch.
+ * Writes a permutation of 0..R-1 to ray_order (R). Pass it to forward and backward. */
+int ever_ray_order(const float* rayo, const float* rayd, int64_t num_rays, void* workspace,
+                   size_t workspace_bytes, int32_t* ray_order, void* stream);
 
 #ifdef __cplusplus
 }

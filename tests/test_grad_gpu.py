@@ -131,6 +131,25 @@ def test_means2d_gradient_single_camera():
     assert _rel_err(g["means2d"], expect) < REPLAY_TOL
 
 
+@pytest.mark.parametrize("order", [None, "auto"])
+def test_gradients_independent_of_launch_order(order):
+    sc = S.uniform_scene(1000, 3, seed=15)
+    ro, rd = S.look_at_rays(S.Camera(np.array([0.0, 0.0, 3.0]), 24, 24, 50.0))
+    dout = np.random.default_rng(15).normal(size=(ro.shape[0], 5))
+    dev = _dev()
+    t = {k: torch.tensor(np.ascontiguousarray(getattr(sc, k), np.float32), device=dev, requires_grad=True)
+         for k in NAMES}
+    rayo = torch.tensor(ro, device=dev, requires_grad=True)
+    rayd = torch.tensor(rd, device=dev, requires_grad=True)
+    out = trace_rays(t["mean"], t["scale"], t["quat"], t["density"], t["features"], rayo, rayd, ray_order=order)
+    (out * torch.tensor(dout, dtype=torch.float32, device=dev)).sum().backward()
+    rep = _oracle_grads(sc, ro, rd, dout, mode="f32_replay")
+    got = {k: v.grad.cpu().double().numpy() for k, v in t.items()}
+    got["rayo"], got["rayd"] = rayo.grad.cpu().double().numpy(), rayd.grad.cpu().double().numpy()
+    for k in rep:
+        assert _rel_err(got[k], _clip(k, rep[k])) < REPLAY_TOL, k
+
+
 def test_truncated_rays_get_no_gradient():
     # backwards_kernel.slang:304: rays with iters >= max_iters - 1 contribute nothing
     sc = S.uniform_scene(1500, 0, seed=14)

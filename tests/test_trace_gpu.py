@@ -32,7 +32,7 @@ def _gpu_trace(sc, ro, rd, tmin=0.0, tmax=1000.0, max_iters=500, sh_degree=None,
     scene = T.Scene(t(sc.mean), t(sc.scale), t(sc.quat), t(np.asarray(sc.density).reshape(-1)), t(sc.features))
     fwd = T.forward(scene, t(ro), t(rd), tmin, tmax, max_iters, sh_degree, log_events=True, touch_count=True,
                     ray_stats=True, tune=tune, ray_order=ray_order)
-    tri = T.reference_tri_collection(scene, fwd, max_iters)
+    tri = T.reference_tri_collection(scene, fwd, max_iters, ray_order)
     torch.cuda.synchronize()
     return scene, fwd, tri.cpu().numpy().reshape(max(max_iters, 0), -1)
 
@@ -153,13 +153,19 @@ def test_empty_and_single():
     assert out.shape == (0, 5)
 
 
-def test_ray_order_permutation_is_transparent():
+@pytest.mark.parametrize("kind", ["random", "coherent"])
+def test_ray_order_permutation_is_transparent(kind):
     sc = S.uniform_scene(2000, 3, seed=9)
     ro, rd = S.look_at_rays(S.Camera(np.array([0.0, 0.0, 3.0]), 32, 32, 50.0))
-    _, a, _ = _gpu_trace(sc, ro, rd)
-    perm = torch.randperm(ro.shape[0], generator=torch.Generator().manual_seed(0)).to(torch.int32).cuda()
-    _, b, _ = _gpu_trace(sc, ro, rd, ray_order=perm)
+    _, a, ta = _gpu_trace(sc, ro, rd)
+    if kind == "random":
+        perm = torch.randperm(ro.shape[0], generator=torch.Generator().manual_seed(0)).to(torch.int32).cuda()
+    else:
+        perm = T.ray_order(torch.tensor(ro, device="cuda"), torch.tensor(rd, device="cuda"))
+        assert torch.equal(torch.sort(perm.long()).values, torch.arange(ro.shape[0], device="cuda"))
+    _, b, tb = _gpu_trace(sc, ro, rd, ray_order=perm)
     assert torch.equal(a.out, b.out) and torch.equal(a.iters, b.iters) and torch.equal(a.states, b.states)
+    assert np.array_equal(ta, tb)
 
 
 def test_deterministic():
