@@ -56,7 +56,7 @@ int64_t ray_order_workspace(int64_t R) {
   c.take(R * 4);
   c.take(R * 4);
   c.take(R * 4);
-  c.take(int64_t(sort_blocks(R)) * 256 * 4);
+  c.take((int64_t(sort_blocks(R)) * 256 + 512) * 4);
   return c.offset;
 }
 
@@ -67,7 +67,7 @@ cudaError_t ray_order(const float* rayo, const float* rayd, int64_t R, char* ws,
   uint32_t* va = reinterpret_cast<uint32_t*>(ws + c.take(R * 4));
   uint32_t* kb = reinterpret_cast<uint32_t*>(ws + c.take(R * 4));
   uint32_t* vb = reinterpret_cast<uint32_t*>(ws + c.take(R * 4));
-  uint32_t* hist = reinterpret_cast<uint32_t*>(ws + c.take(int64_t(sort_blocks(R)) * 256 * 4));
+  uint32_t* hist = reinterpret_cast<uint32_t*>(ws + c.take((int64_t(sort_blocks(R)) * 256 + 512) * 4));
   k_ray_keys<<<unsigned((R + 255) / 256), 256, 0, st>>>(rayo, rayd, R, ka, va);
   sort_pairs(ka, va, kb, vb, hist, R, 30, st);
   return cudaMemcpyAsync(order, va, R * sizeof(int32_t), cudaMemcpyDeviceToDevice, st);

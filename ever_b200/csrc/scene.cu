@@ -163,26 +163,73 @@ __global__ void k_sort_hist(const uint32_t* __restrict__ keys, int64_t N, int sh
   hist[int64_t(threadIdx.x) * nblocks + blockIdx.x] = h[threadIdx.x];
 }
 
-// Exclusive scan of the digit-major histogram (one block of 1024 threads).
-__global__ void k_sort_scan(uint32_t* __restrict__ hist, int64_t len) {
-  __shared__ uint32_t part[1024];
-  const int64_t chunk = (len + 1023) / 1024;
-  const int64_t b = threadIdx.x * chunk, e = min(len, b + chunk);
-  uint32_t s = 0;
-  for (int64_t i = b; i < e; ++i) s += hist[i];
-  part[threadIdx.x] = s;
-  __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {
-    const uint32_t v = threadIdx.x >= off ? part[threadIdx.x - off] : 0u;
-    __syncthreads();
-    part[threadIdx.x] += v;
-    __syncthreads();
+// Exclusive scan of the digit-major histogram in three coalesced kernels: per-chunk
+// sums, a scan of the chunk sums (one block), and a per-chunk scan seeded by it.
+constexpr int kScanChunks = 512;
+constexpr int kScanThreads = 256;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* sh, uint32_t& total) {
+  // sh: kScanThreads / 32 words
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
   }
-  uint32_t run = part[threadIdx.x] - s;
-  for (int64_t i = b; i < e; ++i) {
-    const uint32_t v = hist[i];
-    hist[i] = run;
-    run += v;
+  if (lane == 31) sh[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < kScanThreads / 32 ? sh[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < kScanThreads / 32) sh[lane] = w;
+  }
+  __syncthreads();
+  const uint32_t before = warp > 0 ? sh[warp - 1] : 0u;
+  total = sh[kScanThreads / 32 - 1];
+  __syncthreads();
+  return before + x - v;
+}
+
+__global__ void k_scan_sums(const uint32_t* __restrict__ hist, int64_t len, uint32_t* __restrict__ sums) {
+  const int64_t chunk = (len + kScanChunks - 1) / kScanChunks;
+  const int64_t b = blockIdx.x * chunk, e = min(len, b + chunk);
+  uint32_t s = 0;
+  for (int64_t i = b + threadIdx.x; i < e; i += kScanThreads) s += hist[i];
+  __shared__ uint32_t sh[kScanThreads / 32];
+  uint32_t total;
+  block_exclusive_scan(s, sh, total);
+  if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+__global__ void k_scan_top(uint32_t* __restrict__ sums) {
+  __shared__ uint32_t sh[kScanThreads / 32];
+  uint32_t carry = 0;
+  for (int base = 0; base < kScanChunks; base += kScanThreads) {
+    const uint32_t v = sums[base + threadIdx.x];
+    uint32_t total;
+    const uint32_t ex = block_exclusive_scan(v, sh, total);
+    sums[base + threadIdx.x] = carry + ex;
+    carry += total;
+  }
+}
+
+__global__ void k_scan_chunks(uint32_t* __restrict__ hist, int64_t len, const uint32_t* __restrict__ sums) {
+  const int64_t chunk = (len + kScanChunks - 1) / kScanChunks;
+  const int64_t b = blockIdx.x * chunk, e = min(len, b + chunk);
+  __shared__ uint32_t sh[kScanThreads / 32];
+  uint32_t carry = sums[blockIdx.x];
+  for (int64_t base = b; base < e; base += kScanThreads) {
+    const int64_t i = base + threadIdx.x;
+    const uint32_t v = i < e ? hist[i] : 0u;
+    uint32_t total;
+    const uint32_t ex = block_exclusive_scan(v, sh, total);
+    if (i < e) hist[i] = carry + ex;
+    carry += total;
   }
 }
 
@@ -237,7 +284,7 @@ __global__ void k_sort_scatter(const uint32_t* __restrict__ kin, const uint32_t*
 __global__ void k_gather(const uint32_t* __restrict__ sorted_vals, int64_t N, int K,
                          const float* __restrict__ mean, const float* __restrict__ scale,
                          const float* __restrict__ quat, const float* __restrict__ density,
-                         const float* __restrict__ feat, const float4* __restrict__ aabb_in,
+                         const float4* __restrict__ aabb_in,
                          float4* __restrict__ aabb_out, Record* __restrict__ recs, float* __restrict__ feat_out,
                          int32_t* __restrict__ order) {
   const int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -255,10 +302,17 @@ __global__ void k_gather(const uint32_t* __restrict__ sorted_vals, int64_t N, in
   recs[j] = R;
   aabb_out[2 * j] = aabb_in[2 * p];
   aabb_out[2 * j + 1] = aabb_in[2 * p + 1];
-  const float* src = feat + p * int64_t(K) * 3;
-  float* dst = feat_out + j * int64_t(feat_stride(K));
-  for (int k = 0; k < 3 * K; ++k) dst[k] = src[k];
-  for (int k = 3 * K; k < feat_stride(K); ++k) dst[k] = 0.f;
+}
+
+// Feature rows into Morton order, one thread per padded float (coalesced on both sides).
+__global__ void k_gather_features(const int32_t* __restrict__ order, int64_t N, int K, const float* __restrict__ feat,
+                                  float* __restrict__ feat_out) {
+  const int fst = feat_stride(K);
+  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= N * fst) return;
+  const int64_t j = t / fst;
+  const int k = int(t - j * fst);
+  feat_out[t] = k < 3 * K ? feat[int64_t(order[j]) * 3 * K + k] : 0.f;
 }
 
 __global__ void k_set_features(const int32_t* __restrict__ order, int64_t N, int K, const float* __restrict__ feat,
@@ -373,9 +427,13 @@ int sort_blocks(int64_t N) { return int(div_up(std::max<int64_t>(N, 1), kSortTil
 void sort_pairs(uint32_t*& ka, uint32_t*& va, uint32_t*& kb, uint32_t*& vb, uint32_t* hist, int64_t N, int bits,
                 cudaStream_t st) {
   const int nblocks = sort_blocks(N);
+  const int64_t len = int64_t(nblocks) * 256;
+  uint32_t* sums = hist + len;  // kScanChunks words after the histogram
   for (int shift = 0; shift < bits; shift += 8) {
     k_sort_hist<<<nblocks, kSortThreads, 0, st>>>(ka, N, shift, hist, nblocks);
-    k_sort_scan<<<1, 1024, 0, st>>>(hist, int64_t(nblocks) * 256);
+    k_scan_sums<<<kScanChunks, kScanThreads, 0, st>>>(hist, len, sums);
+    k_scan_top<<<1, kScanThreads, 0, st>>>(sums);
+    k_scan_chunks<<<kScanChunks, kScanThreads, 0, st>>>(hist, len, sums);
     k_sort_scatter<<<nblocks, kSortThreads, 0, st>>>(ka, va, kb, vb, N, shift, hist, nblocks);
     std::swap(ka, kb);
     std::swap(va, vb);
@@ -397,7 +455,7 @@ SceneLayout scene_layout(int64_t N, int K) {
   L.vals_a = c.take(N * sizeof(uint32_t));
   L.vals_b = c.take(N * sizeof(uint32_t));
   L.nblocks = sort_blocks(N);
-  L.hist = c.take(int64_t(L.nblocks) * 256 * sizeof(uint32_t));
+  L.hist = c.take((int64_t(L.nblocks) * 256 + kScanChunks) * sizeof(uint32_t));
   L.parent_node = c.take(std::max<int64_t>(n1, 1) * sizeof(int32_t));
   L.parent_leaf = c.take(std::max<int64_t>(N, 1) * sizeof(int32_t));
   L.flags = c.take(std::max<int64_t>(n1, 1) * sizeof(uint32_t));
@@ -440,8 +498,9 @@ cudaError_t scene_build(const float* mean, const float* scale, const float* quat
   k_morton<<<unsigned(gb), tb, 0, st>>>(aabb_a, N, bounds, ka, va);
   // 30-bit keys: 4 passes of 8 bits
   sort_pairs(ka, va, kb, vb, hist, N, 30, st);
-  k_gather<<<unsigned(gb), tb, 0, st>>>(va, N, K, mean, scale, quat, density, feat, aabb_a, aabb_b,
+  k_gather<<<unsigned(gb), tb, 0, st>>>(va, N, K, mean, scale, quat, density, aabb_a, aabb_b,
                                         reinterpret_cast<Record*>(sc->records), sc->features, sc->order);
+  k_gather_features<<<unsigned(div_up(N * feat_stride(K), tb)), tb, 0, st>>>(sc->order, N, K, feat, sc->features);
   if (N == 1) {
     k_single_leaf<<<1, 1, 0, st>>>(nodes, aabb_b);
     return cudaGetLastError();

@@ -508,9 +508,7 @@ __global__ void k_finalize(const FinalizeParams P) {
   }
   for (int i = 0; i < 4; ++i) P.out.dquat[4 * p + i] = clip_grad(gq[i], 1e3f);
   P.out.ddensity[p] = clip_grad(g[12], 50.f);
-  const int64_t per = int64_t(P.K) * 3;
-  const int64_t fst = feat_stride(P.K);
-  for (int64_t k = 0; k < per; ++k) P.out.dfeatures[p * per + k] = clip_grad(P.acc_feat[j * fst + k], 1e3f);
+
   if (single_wct) {
     const float mx = P.mean[3 * p], my = P.mean[3 * p + 1], mz = P.mean[3 * p + 2];
     const float z = mx * wct[2] + my * wct[6] + mz * wct[10] + wct[14];
@@ -520,6 +518,17 @@ __global__ void k_finalize(const FinalizeParams P) {
 }
 
 // tri[i * R + ray] from log[i * R + slot], ray = ray_order[slot] (or slot).
+// Feature gradients back to original order and shape (N,K,3), clipped at 1e3; one
+// thread per output float.
+__global__ void k_finalize_features(const int32_t* __restrict__ order, int64_t N, int K,
+                                    const float* __restrict__ acc_feat, float* __restrict__ dfeat) {
+  const int64_t per = int64_t(K) * 3;
+  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= N * per) return;
+  const int64_t j = t / per, k = t - j * per;
+  dfeat[int64_t(order[j]) * per + k] = clip_grad(acc_feat[j * feat_stride(K) + k], 1e3f);
+}
+
 __global__ void k_log_to_reference(const int32_t* __restrict__ order, const int32_t* __restrict__ log, int log_cap,
                                    const int32_t* __restrict__ iters, int64_t R, const int32_t* __restrict__ ray_order,
                                    int32_t* __restrict__ tri, int max_iters) {
@@ -561,6 +570,8 @@ cudaError_t launch_backward(const BwdParams& P, int deg, const EverTune& tune, c
 cudaError_t launch_finalize(const FinalizeParams& P, cudaStream_t st) {
   if (P.N == 0) return cudaSuccess;
   k_finalize<<<unsigned((P.N + 255) / 256), 256, 0, st>>>(P);
+  const int64_t total = P.N * int64_t(P.K) * 3;
+  k_finalize_features<<<unsigned((total + 255) / 256), 256, 0, st>>>(P.order, P.N, P.K, P.acc_feat, P.out.dfeatures);
   return cudaGetLastError();
 }
 
