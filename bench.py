@@ -45,6 +45,8 @@ def parse():
     p.add_argument("--kbuf", type=int, default=0)
     p.add_argument("--block", type=int, default=0)
     p.add_argument("--verbose", action="store_true", help="per-step device times on stderr")
+    p.add_argument("--once", action="store_true",
+                   help="one scene build + ray order + forward + backward and exit (for ncu captures)")
     return p.parse_args()
 
 
@@ -179,10 +181,31 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_once(args):
+    """One untimed pass of the hot path through the tracer API: what an ncu capture profiles."""
+    import torch
+    from ever_b200 import tracer as T
+    dev = torch.device("cuda", 0)
+    sc, ro, rd = workload(args)
+    t = lambda a: torch.tensor(np.ascontiguousarray(a), device=dev)
+    rayo, rayd = t(ro), t(rd)
+    tune = T.Tune(kbuf=args.kbuf or 16, block=args.block or 128)
+    scene = T.Scene(t(sc.mean), t(sc.scale), t(sc.quat), t(sc.density.reshape(-1)), t(sc.features))
+    order = T.ray_order(rayo, rayd)
+    fwd = T.forward(scene, rayo, rayd, 0.0, 1000.0, 500, ray_order=order, tune=tune)
+    T.backward(scene, rayo, rayd, fwd, torch.ones((rayo.shape[0], 5), device=dev), 0.0, 1000.0, 500,
+               ray_order=order, tune=tune)
+    torch.cuda.synchronize()
+    print(json.dumps({"once": True, "rays": int(rayo.shape[0]), "status": int(fwd.status.item()),
+                      "events_per_ray": float(fwd.iters.float().mean().item())}))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.once:
+        return run_once(args)
     import torch
     import torch.distributed as dist
 
@@ -195,6 +218,7 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
 
+    from ever_b200 import distributed as D
     from ever_b200 import tracer as T
     from ever_b200.fast_ellipsoid_splinetracer import trace_rays
 
@@ -217,8 +241,7 @@ def main():
                          rayo, rayd, 0.0, 1000.0, 3, None, None, 500, False, None, tune)
         out.backward(gout)
         if world > 1:
-            for p in params.values():
-                dist.all_reduce(p.grad)
+            D.allreduce_gradients([p.grad for p in params.values()])
         return out
 
     for i in range(args.warmup):
@@ -253,30 +276,29 @@ def main():
         for i, m in enumerate(marks):
             print(f"timed step {i}: {prev.elapsed_time(m):.2f} ms", file=sys.stderr, flush=True)
             prev = m
-    ms = ev0.elapsed_time(ev1) / args.steps
-    ms_t = torch.tensor([ms], device=dev)
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms = float(ms_t.item())
+    ms = D.max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dev)
     value = world * R / (ms * 1e-3) / 1e6
 
     # ---- phase breakdown (outside the timed region): build / forward / backward kernels
     def phases(reps=3):
         scene_t = [params[k].detach() for k in ("mean", "scale", "quat", "density", "features")]
-        res = {"build": [], "fwd": [], "bwd": []}
+        res = {"order": [], "build": [], "fwd": [], "bwd": []}
         for _ in range(reps):
-            e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
             e[0].record()
-            scene = T.Scene(*scene_t)
+            order = T.ray_order(rayo, rayd)
             e[1].record()
-            fwd = T.forward(scene, rayo, rayd, 0.0, 1000.0, 500, tune=tune, ray_stats=True)
+            scene = T.Scene(*scene_t)
             e[2].record()
-            T.backward(scene, rayo, rayd, fwd, gout, 0.0, 1000.0, 500, tune=tune)
+            fwd = T.forward(scene, rayo, rayd, 0.0, 1000.0, 500, tune=tune, ray_stats=True, ray_order=order)
             e[3].record()
+            T.backward(scene, rayo, rayd, fwd, gout, 0.0, 1000.0, 500, tune=tune, ray_order=order)
+            e[4].record()
             torch.cuda.synchronize()
-            res["build"].append(e[0].elapsed_time(e[1]))
-            res["fwd"].append(e[1].elapsed_time(e[2]))
-            res["bwd"].append(e[2].elapsed_time(e[3]))
+            res["order"].append(e[0].elapsed_time(e[1]))
+            res["build"].append(e[1].elapsed_time(e[2]))
+            res["fwd"].append(e[2].elapsed_time(e[3]))
+            res["bwd"].append(e[3].elapsed_time(e[4]))
         med = {k: float(np.median(v)) for k, v in res.items()}
         stats = fwd.ray_stats
         med["events_per_ray"] = float(stats[:, 0].mean().item())
@@ -310,11 +332,8 @@ def main():
         e2e_step()
     e1.record()
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / args.steps
-    e2e_t = torch.tensor([e2e_ms], device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_value = world * R / (float(e2e_t.item()) * 1e-3) / 1e6
+    e2e_ms = D.max_over_ranks(e0.elapsed_time(e1) / args.steps, dev)
+    e2e_value = world * R / (e2e_ms * 1e-3) / 1e6
 
     # ---- roofline of the dominant kernel (algorithmic bytes per launch / launch time)
     N = args.prims
@@ -340,8 +359,9 @@ def main():
                    "parallelism": f"rays sharded by view, dp{world}",
                    "l2": "inputs larger than L2 (scene 236 MB + rays 50 MB per step)"},
         "fwd_mrays_trace_only": R / (ph["fwd"] * 1e-3) / 1e6,
-        "fwd_mrays_with_build": R / ((ph["fwd"] + ph["build"]) * 1e-3) / 1e6,
+        "fwd_mrays_with_build": R / ((ph["fwd"] + ph["build"] + ph["order"]) * 1e-3) / 1e6,
         "fwdbwd_mrays_trace_only": R / ((ph["fwd"] + ph["bwd"]) * 1e-3) / 1e6,
+        "fwdbwd_mrays_with_build": R / ((ph["fwd"] + ph["bwd"] + ph["build"] + ph["order"]) * 1e-3) / 1e6,
         "phase_ms": ph,
         "clocks": clk.summary(),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
