@@ -59,6 +59,7 @@ SIGNATURES = {
                                                    c_i32, c_p]),
     "ever_ray_order_workspace_bytes": (c_sz, [c_i64]),
     "ever_ray_order": (ctypes.c_int, [c_p, c_p, c_i64, c_p, c_sz, c_p, c_p]),
+    "ever_ray_order_static": (ctypes.c_int, [c_p, c_p, c_i64, c_p, c_p]),
 }
 
 _lock = threading.Lock()

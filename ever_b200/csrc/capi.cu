@@ -51,6 +51,8 @@ int resolve_degree(const EverScene* sc, const EverTraceArgs* a, int* deg) {
 
 }  // namespace
 
+int ever::set_last_error(int code, const char* msg) { return fail(code, "%s", msg); }
+
 extern "C" {
 
 const char* ever_last_error(void) { return g_last_error.c_str(); }

@@ -9,6 +9,9 @@
 
 namespace ever {
 
+// Records a message for ever_last_error() and returns code (defined in capi.cu).
+int set_last_error(int code, const char* msg);
+
 // Bump allocator over a caller-provided workspace: 256-byte aligned segments.
 struct WsCursor {
   int64_t offset = 0;

@@ -158,6 +158,19 @@ size_t ever_ray_order_workspace_bytes(int64_t num_rays);
 int ever_ray_order(const float* rayo, const float* rayd, int64_t num_rays, void* workspace,
                    size_t workspace_bytes, int32_t* ray_order, void* stream);
 
+/* ever_ray_order for callers that cannot allocate device memory: no workspace argument
+ * and no allocation inside. No counterpart in the reference. Meant for callers such as a
+ * viewer's or render server's frame loop that must never block on the allocator (cudaFree
+ * waits for the whole device), or a binding from another runtime that cannot hand this
+ * library a workspace. Its scratch is a static device array of about 33 MB built into the
+ * library, held by every GPU that loads it until exit; num_rays must be <= 2,097,152 (one
+ * 1920x1080 view), larger counts return EVER_ERR_INVALID. The first call on a device looks
+ * the array's address up (make it before any stream capture); calls that overlap on the
+ * GPU share the array and race, so order them (e.g. one stream). Same output as
+ * ever_ray_order. */
+int ever_ray_order_static(const float* rayo, const float* rayd, int64_t num_rays, int32_t* ray_order,
+                          void* stream);
+
 #ifdef __cplusplus
 }
 #endif
