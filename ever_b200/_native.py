@@ -37,6 +37,17 @@ class EverTraceArgs(ctypes.Structure):
     _fields_ = [("tmin", c_f32), ("tmax", c_f32), ("max_iters", c_i32), ("sh_degree", c_i32)]
 
 
+class EverBatchView(ctypes.Structure):
+    _fields_ = [("scene", c_i32), ("pad", c_i32), ("ray_offset", c_i64), ("ray_count", c_i64)]
+
+
+class EverBatch(ctypes.Structure):
+    _fields_ = [("num_scenes", c_i32), ("num_views", c_i32), ("num_slots", c_i64), ("num_rays", c_i64),
+                ("scene_table", c_p), ("view_table", c_p), ("slot_ray", c_p), ("counters", c_p),
+                ("order_scratch", c_p), ("sh_coeffs", c_i32 * 64), ("num_prims", c_i64 * 64),
+                ("bwd_workspace", c_p * 64)]
+
+
 STATUS_STACK_OVERFLOW = 1
 STATUS_LOG_OVERFLOW = 2
 STATUS_INIT_OVERFLOW = 4
@@ -60,6 +71,18 @@ SIGNATURES = {
     "ever_ray_order_workspace_bytes": (c_sz, [c_i64]),
     "ever_ray_order": (ctypes.c_int, [c_p, c_p, c_i64, c_p, c_sz, c_p, c_p]),
     "ever_ray_order_static": (ctypes.c_int, [c_p, c_p, c_i64, c_p, c_p]),
+    "ever_batch_workspace_bytes": (c_sz, [c_i32, ctypes.POINTER(EverBatchView), c_i32, ctypes.POINTER(c_i64)]),
+    "ever_batch_setup": (ctypes.c_int, [ctypes.POINTER(EverScene), ctypes.POINTER(c_p), c_i32,
+                                        ctypes.POINTER(EverBatchView), c_i32, c_i64, c_p, c_sz,
+                                        ctypes.POINTER(EverBatch)]),
+    "ever_batch_order": (ctypes.c_int, [ctypes.POINTER(EverBatch), c_p, c_p, c_p]),
+    "ever_trace_forward_batched": (ctypes.c_int, [ctypes.POINTER(EverBatch), c_p, c_p, ctypes.POINTER(EverTraceArgs),
+                                                  ctypes.POINTER(EverTune), ctypes.POINTER(EverForwardOut), c_p]),
+    "ever_trace_backward_batched": (ctypes.c_int, [ctypes.POINTER(EverBatch), c_p, c_p,
+                                                   ctypes.POINTER(EverTraceArgs), c_p, c_p, c_p, c_p, c_i32, c_p,
+                                                   c_p, ctypes.POINTER(EverTune), c_p]),
+    "ever_scene_finalize_gradients": (ctypes.c_int, [ctypes.POINTER(EverScene), c_p, c_p, c_p, c_p, c_sz,
+                                                     ctypes.POINTER(EverBackwardOut), c_p]),
 }
 
 _lock = threading.Lock()

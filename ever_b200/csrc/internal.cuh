@@ -35,6 +35,9 @@ int sort_blocks(int64_t N);
 void sort_pairs(uint32_t*& ka, uint32_t*& va, uint32_t*& kb, uint32_t*& vb, uint32_t* hist, int64_t N, int bits,
                 cudaStream_t st);
 int64_t ray_order_workspace(int64_t R);
+struct BatchView;
+cudaError_t batch_ray_order(const float* rayo, const float* rayd, int64_t R, const BatchView* views, int num_views,
+                            char* ws, int32_t* slot_ray, int64_t num_slots, cudaStream_t st);
 cudaError_t ray_order(const float* rayo, const float* rayd, int64_t R, char* ws, int32_t* order, cudaStream_t st);
 cudaError_t scene_build(const float* mean, const float* scale, const float* quat, const float* density,
                         const float* feat, int64_t N, int K, char* ws, const SceneLayout& L, EverScene* sc,
@@ -58,6 +61,70 @@ struct FwdParams {
 };
 
 cudaError_t launch_forward(const FwdParams& P, int deg, const EverTune& tune, cudaStream_t st);
+
+// ---- batched persistent launches: many views over several scenes in one launch ----
+struct BatchScene {  // one row of the device-side scene table
+  const void* nodes;
+  const void* records;
+  const float* features;
+  const int32_t* order;
+  int64_t N;
+  int32_t K;
+  int32_t pad;
+  float* acc_geo;   // backward accumulators of this scene (Morton order)
+  float* acc_feat;
+};
+
+struct BatchView {  // slots [slot_offset, slot_offset + slot_count) belong to one scene
+  int64_t slot_offset;  // a multiple of 32: a warp's packet never mixes views
+  int64_t slot_count;
+  int64_t ray_offset;   // the view's rays in the concatenated arrays
+  int64_t ray_count;
+  int32_t scene;
+  int32_t pad;
+};
+
+struct BatchFwdParams {
+  const BatchScene* scenes;
+  const BatchView* views;
+  int num_views;
+  const int32_t* slot_ray;  // global ray index per slot, -1 for padding
+  int64_t num_slots;
+  const float* rayo;
+  const float* rayd;
+  int64_t R;
+  float tmin, tmax;
+  int max_iters;
+  EverForwardOut out;  // ray-indexed outputs; event_log columns are slots (stride num_slots)
+  unsigned int* work_counter;
+  int grid;            // persistent blocks
+};
+
+cudaError_t launch_forward_batched(const BatchFwdParams& P, int deg, const EverTune& tune, cudaStream_t st);
+
+struct BatchBwdParams {
+  const BatchScene* scenes;
+  const BatchView* views;
+  int num_views;
+  const int32_t* slot_ray;
+  int64_t num_slots;
+  const float* rayo;
+  const float* rayd;
+  int64_t R;
+  float tmin, tmax;
+  int max_iters;
+  const float* grad_out;
+  const float* states;
+  const int32_t* iters;
+  const int32_t* event_log;
+  int log_cap;
+  float* drayo;
+  float* drayd;
+  unsigned int* work_counter;
+  int grid;
+};
+
+cudaError_t launch_backward_batched(const BatchBwdParams& P, int deg, const EverTune& tune, cudaStream_t st);
 
 struct BwdParams {
   const void* nodes;

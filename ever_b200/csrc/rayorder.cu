@@ -48,7 +48,64 @@ __global__ void k_ray_keys(const float* __restrict__ rayo, const float* __restri
   vals[r] = uint32_t(r);
 }
 
+__device__ __forceinline__ int view_of(const BatchView* __restrict__ views, int num_views, int64_t r) {
+  int v = 0;
+  while (v + 1 < num_views && views[v + 1].ray_offset <= r) ++v;
+  return v;
+}
+
+// Batched keys: the view index above the direction's Morton code, so one sort orders every
+// view at once and keeps the views apart.
+__global__ void k_batch_ray_keys(const float* __restrict__ rayd, int64_t R, const BatchView* __restrict__ views,
+                                 int num_views, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  const int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  float dx = rayd[3 * r], dy = rayd[3 * r + 1], dz = rayd[3 * r + 2];
+  const float l1 = fabsf(dx) + fabsf(dy) + fabsf(dz);
+  float u = 0.f, v = 0.f;
+  if (l1 > 0.f && isfinite(l1)) {
+    u = dx / l1;
+    v = dy / l1;
+    if (dz < 0.f) {
+      const float uu = (1.f - fabsf(v)) * (u >= 0.f ? 1.f : -1.f);
+      const float vv = (1.f - fabsf(u)) * (v >= 0.f ? 1.f : -1.f);
+      u = uu;
+      v = vv;
+    }
+  }
+  const uint32_t qu = min(uint32_t(fmaxf(u * 0.5f + 0.5f, 0.f) * 4096.f), 4095u);
+  const uint32_t qv = min(uint32_t(fmaxf(v * 0.5f + 0.5f, 0.f) * 4096.f), 4095u);
+  keys[r] = (uint32_t(view_of(views, num_views, r)) << 24) | (spread2(qu) << 1) | spread2(qv);
+  vals[r] = uint32_t(r);
+}
+
+// Sorted position p of view v lands in slot slot_offset_v + (p - ray_offset_v).
+__global__ void k_batch_fill_slots(const uint32_t* __restrict__ sorted, int64_t R, const BatchView* __restrict__ views,
+                                   int num_views, int32_t* __restrict__ slot_ray) {
+  const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (p >= R) return;
+  const int v = view_of(views, num_views, p);  // views tile the rays in order, so p and its ray share a view
+  slot_ray[views[v].slot_offset + (p - views[v].ray_offset)] = int32_t(sorted[p]);
+}
+
 }  // namespace
+
+cudaError_t batch_ray_order(const float* rayo, const float* rayd, int64_t R, const BatchView* views, int num_views,
+                            char* ws, int32_t* slot_ray, int64_t num_slots, cudaStream_t st) {
+  (void)rayo;
+  cudaError_t e = cudaMemsetAsync(slot_ray, 0xff, num_slots * sizeof(int32_t), st);
+  if (e != cudaSuccess || R == 0) return e;
+  WsCursor c;
+  uint32_t* ka = reinterpret_cast<uint32_t*>(ws + c.take(R * 4));
+  uint32_t* va = reinterpret_cast<uint32_t*>(ws + c.take(R * 4));
+  uint32_t* kb = reinterpret_cast<uint32_t*>(ws + c.take(R * 4));
+  uint32_t* vb = reinterpret_cast<uint32_t*>(ws + c.take(R * 4));
+  uint32_t* hist = reinterpret_cast<uint32_t*>(ws + c.take((int64_t(sort_blocks(R)) * 256 + 512) * 4));
+  k_batch_ray_keys<<<unsigned((R + 255) / 256), 256, 0, st>>>(rayd, R, views, num_views, ka, va);
+  sort_pairs(ka, va, kb, vb, hist, R, 30, st);
+  k_batch_fill_slots<<<unsigned((R + 255) / 256), 256, 0, st>>>(va, R, views, num_views, slot_ray);
+  return cudaGetLastError();
+}
 
 int64_t ray_order_workspace(int64_t R) {
   WsCursor c;

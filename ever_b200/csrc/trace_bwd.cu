@@ -222,10 +222,38 @@ __device__ __forceinline__ float3 sh_basis_vjp(float3 dir, const float* GB) {
 
 __device__ __forceinline__ float clip_grad(float v, float lim) { return v != v ? v : fminf(fmaxf(v, -lim), lim); }
 
+// The scene a ray is traced against, with its gradient accumulators.
+struct BScene {
+  const Node* nodes;
+  const Record* recs;
+  const float* features;
+  int K;
+  float* acc_geo;
+  float* acc_feat;
+};
+
+// Per-launch ray-side inputs and outputs of the backward.
+struct BRayCtx {
+  const float* rayo;
+  const float* rayd;
+  float tmin;
+  int max_iters;
+  const float* grad_out;
+  const float* states;
+  const int32_t* iters;
+  const int32_t* event_log;
+  int64_t log_stride;
+  float* drayo;
+  float* drayd;
+  const float* wct;
+  int num_wct;
+  float* dmeans2d;
+};
+
 // Colour part of one control point's gradient: SH feature gradients (float4 atomics over
 // the 16-byte aligned feature row), G_B for the ray direction; returns dL/d density.
 template <int DEG>
-__device__ __forceinline__ float colour_grads(const BwdParams& P, int j, float dh, float sign, float3 c, float4 Gd,
+__device__ __forceinline__ float colour_grads(const BScene& P, int j, float dh, float sign, float3 c, float4 Gd,
                                               const float* B, float* GB) {
   constexpr int NB = (DEG + 1) * (DEG + 1);
   constexpr int NV = (3 * NB + 3) / 4;
@@ -255,14 +283,9 @@ __device__ __forceinline__ float colour_grads(const BwdParams& P, int j, float d
   return sign * g_dh;
 }
 
+// Reverse replay of ray r (event-log column `slot`) against scene S.
 template <int DEG>
-__global__ void __launch_bounds__(256) k_trace_bwd(const BwdParams P) {
-  extern __shared__ int smem[];
-  const int tid = threadIdx.x, stride = blockDim.x;
-  int* st_node = smem + tid;
-  const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;
-  if (gi >= P.R) return;
-  const int64_t r = P.ray_order ? int64_t(P.ray_order[gi]) : gi;
+__device__ void backward_ray(const BScene& S, const BRayCtx& P, int64_t r, int64_t slot, int* st_node, int stride) {
   const int n = P.iters[r];
   float* gro = P.drayo + 3 * r;
   float* grd = P.drayd + 3 * r;
@@ -271,14 +294,14 @@ __global__ void __launch_bounds__(256) k_trace_bwd(const BwdParams P) {
     grd[0] = grd[1] = grd[2] = 0.f;
     return;
   }
-  const Node* nodes = reinterpret_cast<const Node*>(P.nodes);
-  const Record* recs = reinterpret_cast<const Record*>(P.records);
+  const Node* nodes = S.nodes;
+  const Record* recs = S.recs;
   const float3 ro = make_float3(P.rayo[3 * r], P.rayo[3 * r + 1], P.rayo[3 * r + 2]);
   const float3 rd = make_float3(P.rayd[3 * r], P.rayd[3 * r + 1], P.rayd[3 * r + 2]);
   const Ray ray = make_ray(ro, rd, P.tmin);
   float B[16];
   sh_basis<DEG>(ray.rd, B);
-  const int64_t fstride = feat_stride(P.K);
+  const int64_t fstride = feat_stride(S.K);
 
   // per-ray camera matrix for dmeans2d (backwards_kernel.slang:313-321)
   const bool per_ray_wct = P.wct && P.num_wct > 1 && P.dmeans2d;
@@ -317,11 +340,11 @@ __global__ void __launch_bounds__(256) k_trace_bwd(const BwdParams P) {
 #pragma unroll
   for (int k = 0; k < 16; ++k) GB[k] = 0.f;
 
-  Ctrl cur = load_ctrl<DEG>(recs, P.features, fstride, ray, B, P.event_log[int64_t(n - 1) * P.R + gi]);
+  Ctrl cur = load_ctrl<DEG>(recs, S.features, fstride, ray, B, P.event_log[int64_t(n - 1) * P.log_stride + slot]);
   for (int i = n - 1; i >= 0; --i) {
     Ctrl old;
     if (i > 0) {
-      old = load_ctrl<DEG>(recs, P.features, fstride, ray, B, P.event_log[int64_t(i - 1) * P.R + gi]);
+      old = load_ctrl<DEG>(recs, S.features, fstride, ray, B, P.event_log[int64_t(i - 1) * P.log_stride + slot]);
     } else {
       old.t = 0.f;
       old.dirac = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -336,7 +359,7 @@ __global__ void __launch_bounds__(256) k_trace_bwd(const BwdParams P) {
     const int j = cur.j;
     const Record R = load_record(recs, j);
     const float sign = cur.entry ? 1.f : -1.f;
-    const float g_sigma = colour_grads<DEG>(P, j, sign * R.r3.x, sign, cur.c, Gd, B, GB);
+    const float g_sigma = colour_grads<DEG>(S, j, sign * R.r3.x, sign, cur.c, Gd, B, GB);
     // event time: root of |ocn + t rdn|^2 = 1. dt = -(P.docn + t P.drdn) / (P.rdn) with the
     // hit point in the cancellation-free form P = l +- (sqrt(h)/a) rdn and P.rdn = +-sqrt(h)
     FullHit H;
@@ -393,7 +416,7 @@ __global__ void __launch_bounds__(256) k_trace_bwd(const BwdParams P) {
       }
     }
     // W (9), mean (3), density (1): four float4 atomics
-    float4* ag = reinterpret_cast<float4*>(P.acc_geo + int64_t(j) * kGeo);
+    float4* ag = reinterpret_cast<float4*>(S.acc_geo + int64_t(j) * kGeo);
     atomicAdd(ag + 0, make_float4(gW[0], gW[1], gW[2], gW[3]));
     atomicAdd(ag + 1, make_float4(gW[4], gW[5], gW[6], gW[7]));
     atomicAdd(ag + 2, make_float4(gW[8], -gmu[0], -gmu[1], -gmu[2]));
@@ -422,9 +445,9 @@ __global__ void __launch_bounds__(256) k_trace_bwd(const BwdParams P) {
           const Record R = load_record(recs, j);
           HitT H;
           if (intersect(R, ray, H) && H.t0 <= 0.f && H.t1 > 0.f) {
-            const float3 col = sh_colour<DEG>(P.features + j * fstride, B);
-            const float g_sigma = colour_grads<DEG>(P, j, R.r3.x, 1.f, col, G.drgb, B, GB);
-            atomicAdd(P.acc_geo + int64_t(j) * kGeo + 12, g_sigma);
+            const float3 col = sh_colour<DEG>(S.features + j * fstride, B);
+            const float g_sigma = colour_grads<DEG>(S, j, R.r3.x, 1.f, col, G.drgb, B, GB);
+            atomicAdd(S.acc_geo + int64_t(j) * kGeo + 12, g_sigma);
           }
         }
       }
@@ -457,6 +480,45 @@ __global__ void __launch_bounds__(256) k_trace_bwd(const BwdParams P) {
   grd[0] = clip_grad(g_rd.x, 1e3f);
   grd[1] = clip_grad(g_rd.y, 1e3f);
   grd[2] = clip_grad(g_rd.z, 1e3f);
+}
+
+template <int DEG>
+__global__ void __launch_bounds__(256) k_trace_bwd(const BwdParams P) {
+  extern __shared__ int smem[];
+  const int tid = threadIdx.x;
+  const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;
+  if (gi >= P.R) return;
+  const int64_t r = P.ray_order ? int64_t(P.ray_order[gi]) : gi;
+  const BScene S{reinterpret_cast<const Node*>(P.nodes), reinterpret_cast<const Record*>(P.records), P.features, P.K,
+                 P.acc_geo, P.acc_feat};
+  const BRayCtx C{P.rayo, P.rayd, P.tmin, P.max_iters, P.grad_out, P.states, P.iters, P.event_log, P.R,
+                  P.drayo, P.drayd, P.wct, P.num_wct, P.dmeans2d};
+  backward_ray<DEG>(S, C, r, gi, smem + tid, blockDim.x);
+}
+
+// Persistent batched backward: warps take 32-slot packets from a device counter.
+template <int DEG>
+__global__ void __launch_bounds__(256) k_trace_bwd_batched(const BatchBwdParams P) {
+  extern __shared__ int smem[];
+  const int tid = threadIdx.x, lane = tid & 31;
+  const BRayCtx C{P.rayo, P.rayd, P.tmin, P.max_iters, P.grad_out, P.states, P.iters, P.event_log, P.num_slots,
+                  P.drayo, P.drayd, nullptr, 0, nullptr};
+  const int64_t num_packets = P.num_slots / 32;
+  for (;;) {
+    unsigned int pk = 0;
+    if (lane == 0) pk = atomicAdd(P.work_counter, 1u);
+    pk = __shfl_sync(0xffffffffu, pk, 0);
+    if (int64_t(pk) >= num_packets) break;
+    const int64_t slot = int64_t(pk) * 32 + lane;
+    int v = 0;
+    while (v + 1 < P.num_views && P.views[v + 1].slot_offset <= int64_t(pk) * 32) ++v;
+    const BatchScene bs_ = P.scenes[P.views[v].scene];
+    const BScene S{reinterpret_cast<const Node*>(bs_.nodes), reinterpret_cast<const Record*>(bs_.records),
+                   bs_.features, bs_.K, bs_.acc_geo, bs_.acc_feat};
+    const int32_t r = P.slot_ray[slot];
+    if (r >= 0) backward_ray<DEG>(S, C, r, slot, smem + tid, blockDim.x);
+    __syncwarp();
+  }
 }
 
 // VJP of rotate_vector(v, q) w.r.t. q.
@@ -548,13 +610,38 @@ template <int DEG>
 cudaError_t launch_b(const BwdParams& P, int block, cudaStream_t st) {
   const size_t smem = size_t(kStackDepth) * block * sizeof(int);
   auto kern = k_trace_bwd<DEG>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  cudaError_t e = cudaSuccess;
+  if (smem > 48 * 1024) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   kern<<<unsigned((P.R + block - 1) / block), block, smem, st>>>(P);
   return cudaGetLastError();
 }
 
 }  // namespace
+
+template <int DEG>
+cudaError_t launch_bb(const BatchBwdParams& P, int block, cudaStream_t st) {
+  const size_t smem = size_t(kStackDepth) * block * sizeof(int);
+  auto kern = k_trace_bwd_batched<DEG>;
+  cudaError_t e = cudaSuccess;
+  if (smem > 48 * 1024) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(P.work_counter, 0, sizeof(unsigned int), st);
+  if (e != cudaSuccess) return e;
+  kern<<<P.grid, block, smem, st>>>(P);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_backward_batched(const BatchBwdParams& P, int deg, const EverTune& tune, cudaStream_t st) {
+  if (P.num_slots == 0) return cudaSuccess;
+  const int block = tune.block > 0 ? tune.block : 128;
+  switch (deg) {
+    case 0: return launch_bb<0>(P, block, st);
+    case 1: return launch_bb<1>(P, block, st);
+    case 2: return launch_bb<2>(P, block, st);
+    default: return launch_bb<3>(P, block, st);
+  }
+}
 
 cudaError_t launch_backward(const BwdParams& P, int deg, const EverTune& tune, cudaStream_t st) {
   if (P.R == 0) return cudaSuccess;

@@ -271,13 +271,28 @@ __device__ int point_members(const Node* __restrict__ nodes, const Record* __res
   return n_mem;
 }
 
+// Which scene a packet traces, and the per-launch constants.
+struct SceneRef {
+  const Node* nodes;
+  const Record* recs;
+  const float* features;
+  int64_t N;
+  int K;
+};
+
+struct TraceCtx {
+  float tmin, tmax;
+  int max_iters;
+  int64_t log_stride;  // event-log row length (slots)
+  EverForwardOut out;
+};
+
 // Integrates the gathered events in order. Returns true once the ray is finished.
 template <int KBUF, int DEG>
-__device__ __forceinline__ bool consume(const FwdParams& P, const Record* __restrict__ recs, const Ray& ray,
-                                        const float* B, int bs, int64_t slot, uint64_t (&buf)[KBUF], State& s,
-                                        float4& last_dirac, int& iters, float& s16, int& cnt16, uint64_t& lower,
-                                        uint32_t& status) {
-  const int fst = feat_stride(P.K);
+__device__ __forceinline__ bool consume(const SceneRef& sc, const TraceCtx& C, const Ray& ray, const float* B,
+                                        int bs, int64_t slot, uint64_t (&buf)[KBUF], State& s, float4& last_dirac,
+                                        int& iters, float& s16, int& cnt16, uint64_t& lower, uint32_t& status) {
+  const int fst = feat_stride(sc.K);
   const uint64_t last = buf[KBUF - 1];
   bool done = false;
   for (int n = 0; n < KBUF && !done; ++n) {
@@ -291,30 +306,30 @@ __device__ __forceinline__ bool consume(const FwdParams& P, const Record* __rest
     const int ex = key_exit(k);
     if (!(t > s16)) continue;  // tied with the 16th event of a reference round: dropped
     if (t > kSentinel) return true;
-    const float4 r3 = __ldg(&recs[j].r3);
-    if (ex && t > P.tmax) {
+    const float4 r3 = __ldg(&sc.recs[j].r3);
+    if (ex && t > C.tmax) {
       HitT H;
-      intersect(load_record(recs, j), ray, H);
-      if (!(H.t0 > s16 && H.t0 <= P.tmax)) continue;
+      intersect(load_record(sc.recs, j), ray, H);
+      if (!(H.t0 > s16 && H.t0 <= C.tmax)) continue;
     }
-    const float3 c = sh_colour<DEG>(P.features + int64_t(j) * fst, B, bs);
+    const float3 c = sh_colour<DEG>(sc.features + int64_t(j) * fst, B, bs);
     const float dh = ex ? -r3.x : r3.x;
     const float4 dirac = make_float4(dh, dh * c.x, dh * c.y, dh * c.z);
     update(s, t, dirac);
     last_dirac = dirac;
-    if (P.out.event_log) {
-      if (iters < P.out.log_cap)
-        P.out.event_log[int64_t(iters) * P.R + slot] = 2 * j + (ex ? 0 : 1);
+    if (C.out.event_log) {
+      if (iters < C.out.log_cap)
+        C.out.event_log[int64_t(iters) * C.log_stride + slot] = 2 * j + (ex ? 0 : 1);
       else
         status |= EVER_STATUS_LOG_OVERFLOW;
     }
-    if (P.out.touch_count) atomicAdd(P.out.touch_count + __float_as_int(r3.y), 1);
+    if (C.out.touch_count) atomicAdd(C.out.touch_count + __float_as_int(r3.y), 1);
     ++iters;
     if (++cnt16 == kRefRound) {
       s16 = t;
       cnt16 = 0;
     }
-    if (!(s.logT < kLogCutoff && iters < P.max_iters)) done = true;
+    if (!(s.logT < kLogCutoff && iters < C.max_iters)) done = true;
   }
   if (done || last == kEmptyKey) return true;
   lower = last;
@@ -322,14 +337,14 @@ __device__ __forceinline__ bool consume(const FwdParams& P, const Record* __rest
 }
 
 template <int DEG>
-__device__ __forceinline__ void init_density(const FwdParams& P, const Record* recs, const float* B, int bs, int n_mem,
+__device__ __forceinline__ void init_density(const SceneRef& sc, const float* B, int bs, int n_mem,
                                              const int (&mem_j)[kMaxMembers], float4 extra, uint32_t status,
                                              State& s) {
-  const int fst = feat_stride(P.K);
+  const int fst = feat_stride(sc.K);
   for (int q = 0; q < n_mem; ++q) {
     const int j = mem_j[q];
-    const float sg = __ldg(&recs[j].r3.x);
-    const float3 c = sh_colour<DEG>(P.features + int64_t(j) * fst, B, bs);
+    const float sg = __ldg(&sc.recs[j].r3.x);
+    const float3 c = sh_colour<DEG>(sc.features + int64_t(j) * fst, B, bs);
     s.drgb.x = s.drgb.x + sg;
     s.drgb.y = s.drgb.y + sg * c.x;
     s.drgb.z = s.drgb.z + sg * c.y;
@@ -343,34 +358,39 @@ __device__ __forceinline__ void init_density(const FwdParams& P, const Record* r
   }
 }
 
-__device__ __forceinline__ void write_outputs(const FwdParams& P, int64_t r, const State& s, float4 last_dirac,
+__device__ __forceinline__ void write_outputs(const EverForwardOut& out, int64_t r, const State& s, float4 last_dirac,
                                               int iters, uint32_t status) {
-  float* o = P.out.out + 5 * r;
+  float* o = out.out + 5 * r;
   o[0] = s.C.x;
   o[1] = s.C.y;
   o[2] = s.C.z;
   o[3] = 1.f - expf(-s.logT);
   o[4] = s.dist_x - s.dist_y;
-  if (P.out.states) {
-    float4* st = reinterpret_cast<float4*>(P.out.states + 16 * r);
+  if (out.states) {
+    float4* st = reinterpret_cast<float4*>(out.states + 16 * r);
     st[0] = make_float4(s.dist_x, s.dist_y, s.cum_x, s.cum_y);
     st[1] = make_float4(0.f, 0.f, 0.f, s.t);
     st[2] = s.drgb;
     st[3] = make_float4(s.logT, s.C.x, s.C.y, s.C.z);
   }
-  if (P.out.last_dirac) reinterpret_cast<float4*>(P.out.last_dirac)[r] = last_dirac;
-  P.out.iters[r] = iters;
-  if (P.out.ray_stats) {
-    P.out.ray_stats[2 * r] = float(iters);
-    P.out.ray_stats[2 * r + 1] = s.t;
+  if (out.last_dirac) reinterpret_cast<float4*>(out.last_dirac)[r] = last_dirac;
+  out.iters[r] = iters;
+  if (out.ray_stats) {
+    out.ray_stats[2 * r] = float(iters);
+    out.ray_stats[2 * r + 1] = s.t;
   }
-  if (status && P.out.status) atomicOr(P.out.status, int(status));
+  if (status && out.status) atomicOr(out.status, int(status));
 }
 
-__device__ __forceinline__ Ray load_ray(const FwdParams& P, int64_t r) {
-  const float3 ro = make_float3(P.rayo[3 * r], P.rayo[3 * r + 1], P.rayo[3 * r + 2]);
-  const float3 rd = make_float3(P.rayd[3 * r], P.rayd[3 * r + 1], P.rayd[3 * r + 2]);
-  return make_ray(ro, rd, P.tmin);
+__device__ __forceinline__ Ray load_ray(const float* rayo, const float* rayd, int64_t r, float tmin) {
+  const float3 ro = make_float3(rayo[3 * r], rayo[3 * r + 1], rayo[3 * r + 2]);
+  const float3 rd = make_float3(rayd[3 * r], rayd[3 * r + 1], rayd[3 * r + 2]);
+  return make_ray(ro, rd, tmin);
+}
+
+__device__ __forceinline__ SceneRef scene_of(const FwdParams& P) {
+  return SceneRef{reinterpret_cast<const Node*>(P.nodes), reinterpret_cast<const Record*>(P.records), P.features,
+                  P.N, P.K};
 }
 
 template <int KBUF, int DEG>
@@ -382,9 +402,9 @@ __global__ void __launch_bounds__(256) k_trace_fwd_ray(const FwdParams P) {
   const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;
   if (gi >= P.R) return;
   const int64_t r = P.ray_order ? int64_t(P.ray_order[gi]) : gi;
-  const Node* nodes = reinterpret_cast<const Node*>(P.nodes);
-  const Record* recs = reinterpret_cast<const Record*>(P.records);
-  const Ray ray = load_ray(P, r);
+  const SceneRef sc = scene_of(P);
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out};
+  const Ray ray = load_ray(P.rayo, P.rayd, r, P.tmin);
   const RaySlab sl = make_slab(ray);
   float B[16];
   sh_basis<DEG>(ray.rd, B);
@@ -392,40 +412,34 @@ __global__ void __launch_bounds__(256) k_trace_fwd_ray(const FwdParams P) {
   State s = empty_state();
   float4 last_dirac = make_float4(0.f, 0.f, 0.f, 0.f);
   int iters = 0;
-  if (P.N > 0) {
+  if (sc.N > 0) {
     int mem_p[kMaxMembers], mem_j[kMaxMembers];
     float4 extra = make_float4(0.f, 0.f, 0.f, 0.f);
-    const int n_mem = point_members<DEG, false>(nodes, recs, P.features, feat_stride(P.K), B, 1, ray, true, st_node,
-                                                stride, 0, mem_p, mem_j, extra, status);
-    init_density<DEG>(P, recs, B, 1, n_mem, mem_j, extra, status, s);
+    const int n_mem = point_members<DEG, false>(sc.nodes, sc.recs, sc.features, feat_stride(sc.K), B, 1, ray, true,
+                                                st_node, stride, 0, mem_p, mem_j, extra, status);
+    init_density<DEG>(sc, B, 1, n_mem, mem_j, extra, status, s);
     float s16 = 0.f;
     int cnt16 = 0;
     uint64_t lower = 0;
-    bool done = P.max_iters <= 0;
+    bool done = C.max_iters <= 0;
     while (!done) {
       uint64_t buf[KBUF];
 #pragma unroll
       for (int i = 0; i < KBUF; ++i) buf[i] = kEmptyKey;
-      gather_ray<KBUF>(nodes, recs, ray, sl, lower, s16, P.tmax, buf, st_node, st_t, stride, status);
-      done = consume<KBUF, DEG>(P, recs, ray, B, 1, gi, buf, s, last_dirac, iters, s16, cnt16, lower, status);
+      gather_ray<KBUF>(sc.nodes, sc.recs, ray, sl, lower, s16, C.tmax, buf, st_node, st_t, stride, status);
+      done = consume<KBUF, DEG>(sc, C, ray, B, 1, gi, buf, s, last_dirac, iters, s16, cnt16, lower, status);
     }
   }
-  write_outputs(P, r, s, last_dirac, iters, status);
+  write_outputs(C.out, r, s, last_dirac, iters, status);
 }
 
+// One warp traces one packet of up to 32 rays against one scene (lanes with valid=false
+// only take part in the warp-wide votes).
 template <int KBUF, int DEG>
-__global__ void __launch_bounds__(256) k_trace_fwd_packet(const FwdParams P) {
-  extern __shared__ int smem[];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  int* wstack = smem + warp * kStackDepth;
-  float* B = reinterpret_cast<float*>(smem + (blockDim.x / 32) * kStackDepth) + tid;  // B[k * blockDim.x]
-  const int bs = blockDim.x;
-  const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;
-  const bool valid = gi < P.R;  // every lane stays for the warp-wide ballots
-  const int64_t r = valid ? (P.ray_order ? int64_t(P.ray_order[gi]) : gi) : 0;
-  const Node* nodes = reinterpret_cast<const Node*>(P.nodes);
-  const Record* recs = reinterpret_cast<const Record*>(P.records);
-  const Ray ray = load_ray(P, r);
+__device__ __forceinline__ void trace_packet(const SceneRef& sc, const TraceCtx& C, const float* rayo,
+                                             const float* rayd, int64_t r, bool valid, int64_t slot, int* wstack,
+                                             float* B, int bs, int lane) {
+  const Ray ray = load_ray(rayo, rayd, valid ? r : 0, C.tmin);
   const RaySlab sl = make_slab(ray);
   {
     float Bl[16];
@@ -437,25 +451,65 @@ __global__ void __launch_bounds__(256) k_trace_fwd_packet(const FwdParams P) {
   State s = empty_state();
   float4 last_dirac = make_float4(0.f, 0.f, 0.f, 0.f);
   int iters = 0;
-  if (P.N > 0) {
+  if (sc.N > 0) {
     int mem_p[kMaxMembers], mem_j[kMaxMembers];
     float4 extra = make_float4(0.f, 0.f, 0.f, 0.f);
-    const int n_mem = point_members<DEG, true>(nodes, recs, P.features, feat_stride(P.K), B, bs, ray, valid, wstack,
-                                               1, lane, mem_p, mem_j, extra, status);
-    init_density<DEG>(P, recs, B, bs, n_mem, mem_j, extra, status, s);
+    const int n_mem = point_members<DEG, true>(sc.nodes, sc.recs, sc.features, feat_stride(sc.K), B, bs, ray, valid,
+                                               wstack, 1, lane, mem_p, mem_j, extra, status);
+    init_density<DEG>(sc, B, bs, n_mem, mem_j, extra, status, s);
     float s16 = 0.f;
     int cnt16 = 0;
     uint64_t lower = 0;
-    bool act = valid && P.max_iters > 0;
+    bool act = valid && C.max_iters > 0;
     while (__any_sync(kFull, act)) {
       uint64_t buf[KBUF];
 #pragma unroll
       for (int i = 0; i < KBUF; ++i) buf[i] = kEmptyKey;
-      gather_packet<KBUF>(nodes, recs, ray, sl, act, lower, s16, P.tmax, buf, wstack, lane, status);
-      if (act) act = !consume<KBUF, DEG>(P, recs, ray, B, bs, gi, buf, s, last_dirac, iters, s16, cnt16, lower, status);
+      gather_packet<KBUF>(sc.nodes, sc.recs, ray, sl, act, lower, s16, C.tmax, buf, wstack, lane, status);
+      if (act) act = !consume<KBUF, DEG>(sc, C, ray, B, bs, slot, buf, s, last_dirac, iters, s16, cnt16, lower, status);
     }
   }
-  if (valid) write_outputs(P, r, s, last_dirac, iters, status);
+  if (valid) write_outputs(C.out, r, s, last_dirac, iters, status);
+  __syncwarp();
+}
+
+template <int KBUF, int DEG>
+__global__ void __launch_bounds__(256) k_trace_fwd_packet(const FwdParams P) {
+  extern __shared__ int smem[];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int* wstack = smem + warp * kStackDepth;
+  float* B = reinterpret_cast<float*>(smem + (blockDim.x / 32) * kStackDepth) + tid;  // B[k * blockDim.x]
+  const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;
+  const bool valid = gi < P.R;  // every lane stays for the warp-wide ballots
+  const int64_t r = valid ? (P.ray_order ? int64_t(P.ray_order[gi]) : gi) : 0;
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out};
+  trace_packet<KBUF, DEG>(scene_of(P), C, P.rayo, P.rayd, r, valid, gi, wstack, B, blockDim.x, lane);
+}
+
+// Persistent batched forward: warps take 32-slot packets from a device counter until
+// all views are done. Each packet lies inside one view, hence one scene.
+template <int KBUF, int DEG>
+__global__ void __launch_bounds__(256) k_trace_fwd_batched(const BatchFwdParams P) {
+  extern __shared__ int smem[];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int* wstack = smem + warp * kStackDepth;
+  float* B = reinterpret_cast<float*>(smem + (blockDim.x / 32) * kStackDepth) + tid;
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.num_slots, P.out};
+  const int64_t num_packets = P.num_slots / 32;
+  for (;;) {
+    unsigned int pk = 0;
+    if (lane == 0) pk = atomicAdd(P.work_counter, 1u);
+    pk = __shfl_sync(kFull, pk, 0);
+    if (int64_t(pk) >= num_packets) break;
+    const int64_t slot = int64_t(pk) * 32 + lane;
+    int v = 0;  // the view holding this packet (few views: linear scan, warp-uniform)
+    while (v + 1 < P.num_views && P.views[v + 1].slot_offset <= int64_t(pk) * 32) ++v;
+    const BatchScene bs_ = P.scenes[P.views[v].scene];
+    const SceneRef sc{reinterpret_cast<const Node*>(bs_.nodes), reinterpret_cast<const Record*>(bs_.records),
+                      bs_.features, bs_.N, bs_.K};
+    const int32_t r = P.slot_ray[slot];
+    trace_packet<KBUF, DEG>(sc, C, P.rayo, P.rayd, r, r >= 0, slot, wstack, B, blockDim.x, lane);
+  }
 }
 
 template <int KBUF, int DEG>
@@ -484,7 +538,36 @@ cudaError_t launch_k(const FwdParams& P, int deg, int block, int traversal, cuda
   }
 }
 
+template <int KBUF, int DEG>
+cudaError_t launch_batched_t(const BatchFwdParams& P, int block, cudaStream_t st) {
+  const size_t smem = size_t(kStackDepth) * (block / 32) * sizeof(int) + size_t(16) * block * sizeof(float);
+  cudaError_t e = cudaMemsetAsync(P.work_counter, 0, sizeof(unsigned int), st);
+  if (e != cudaSuccess) return e;
+  k_trace_fwd_batched<KBUF, DEG><<<P.grid, block, smem, st>>>(P);
+  return cudaGetLastError();
+}
+
+template <int KBUF>
+cudaError_t launch_batched_k(const BatchFwdParams& P, int deg, int block, cudaStream_t st) {
+  switch (deg) {
+    case 0: return launch_batched_t<KBUF, 0>(P, block, st);
+    case 1: return launch_batched_t<KBUF, 1>(P, block, st);
+    case 2: return launch_batched_t<KBUF, 2>(P, block, st);
+    default: return launch_batched_t<KBUF, 3>(P, block, st);
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_forward_batched(const BatchFwdParams& P, int deg, const EverTune& tune, cudaStream_t st) {
+  if (P.num_slots == 0) return cudaSuccess;
+  const int block = tune.block > 0 ? tune.block : 128;
+  switch (tune.kbuf) {
+    case 8: return launch_batched_k<8>(P, deg, block, st);
+    case 32: return launch_batched_k<32>(P, deg, block, st);
+    default: return launch_batched_k<16>(P, deg, block, st);
+  }
+}
 
 cudaError_t launch_forward(const FwdParams& P, int deg, const EverTune& tune, cudaStream_t st) {
   if (P.R == 0) return cudaSuccess;

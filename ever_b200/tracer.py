@@ -80,6 +80,18 @@ class Scene:
                                          N.ptr(self.workspace), int(self.workspace.numel()), ctypes.byref(self.c),
                                          _stream(device)))
 
+    def rebuild(self):
+        """Rebuilds the BVH and records in place from the (possibly updated) input tensors.
+
+        The workspace and every device pointer of the scene stay the same, so launches
+        recorded in a CUDA graph keep working across rebuilds.
+        """
+        m, s, q, d, f = self.tensors
+        with torch.cuda.device(self.device):
+            N.check(N.load().ever_scene_build(N.ptr(m), N.ptr(s), N.ptr(q), N.ptr(d), N.ptr(f), self.num_prims,
+                                              self.sh_coeffs, N.ptr(self.workspace), int(self.workspace.numel()),
+                                              ctypes.byref(self.c), _stream(self.device)))
+
     def set_features(self, features):
         _check_tensor("colors", features, self.device, 3)
         if features.shape[0] != self.num_prims or features.shape[1] != self.sh_coeffs:

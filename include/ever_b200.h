@@ -171,6 +171,70 @@ int ever_ray_order(const float* rayo, const float* rayd, int64_t num_rays, void*
 int ever_ray_order_static(const float* rayo, const float* rayd, int64_t num_rays, int32_t* ray_order,
                           void* stream);
 
+/* ---- batched persistent tracing (many views over several scenes per launch) ----
+ * No counterpart in the reference, which launches OptiX once per view. A batch lists
+ * views (a range of rays traced against one built scene). Each view's rays get their own
+ * coherent order and are padded to whole 32-ray packets, so a warp's packet never mixes
+ * scenes; persistent warps take packets from a device counter in packet order. */
+typedef struct EverBatchView {
+  int32_t scene;      /* index into the scenes array given to ever_batch_setup */
+  int32_t pad;
+  int64_t ray_offset; /* first ray of the view in the concatenated ray arrays */
+  int64_t ray_count;
+} EverBatchView;
+
+typedef struct EverBatch {  /* filled by ever_batch_setup; plain data */
+  int32_t num_scenes;
+  int32_t num_views;
+  int64_t num_slots;  /* padded packet slots: event-log columns of a batched forward */
+  int64_t num_rays;
+  void* scene_table;  /* device: one row per scene (pointers into the built scenes) */
+  void* view_table;   /* device: one row per view */
+  int32_t* slot_ray;  /* device (num_slots): ray index per slot, -1 for padding */
+  uint32_t* counters; /* device: work counters of the persistent launches */
+  void* order_scratch;/* device: ray-order sort scratch */
+  int32_t sh_coeffs[64]; /* host copy: K of each scene */
+  int64_t num_prims[64]; /* host copy: N of each scene */
+  void* bwd_workspace[64];/* host copy: backward workspace of each scene (or NULL) */
+} EverBatch;
+
+/* Bytes of batch workspace for these views (host array); *num_slots receives the padded
+ * slot count. At most 64 views and 64 scenes; the views must tile the concatenated rays
+ * in order (view v starts where view v-1 ends, the first at ray 0). */
+size_t ever_batch_workspace_bytes(int32_t num_scenes, const EverBatchView* views, int32_t num_views,
+                                  int64_t* num_slots);
+
+/* Lays the batch out in `workspace` and uploads the scene and view tables. scenes: host
+ * array of built scenes; bwd_workspaces: host array of per-scene backward workspaces
+ * (ever_backward_workspace_bytes each; entries may be NULL for forward-only use). This
+ * set-up call copies the tables synchronously; later calls only enqueue work. */
+int ever_batch_setup(const EverScene* scenes, void* const* bwd_workspaces, int32_t num_scenes,
+                     const EverBatchView* views, int32_t num_views, int64_t num_rays, void* workspace,
+                     size_t workspace_bytes, EverBatch* batch);
+
+/* Coherent order inside every view (ever_ray_order per view), written to the slot map. */
+int ever_batch_order(const EverBatch* batch, const float* rayo, const float* rayd, void* stream);
+
+/* One persistent forward launch over all views. Outputs are indexed by ray; event_log
+ * has log_cap rows of batch->num_slots columns. The scenes must share an SH degree
+ * (args->sh_degree, or sqrt(K)-1 of the first scene). */
+int ever_trace_forward_batched(const EverBatch* batch, const float* rayo, const float* rayd,
+                               const EverTraceArgs* args, const EverTune* tune, const EverForwardOut* out,
+                               void* stream);
+
+/* One persistent backward launch over all views: accumulates every scene's gradients into
+ * its backward workspace (zeroed here) and writes the ray gradients (clipped). */
+int ever_trace_backward_batched(const EverBatch* batch, const float* rayo, const float* rayd,
+                                const EverTraceArgs* args, const float* grad_out, const float* states,
+                                const int32_t* iters, const int32_t* event_log, int32_t log_cap, float* drayo,
+                                float* drayd, const EverTune* tune, void* stream);
+
+/* Turns one scene's accumulated gradients (its backward workspace) into dmean, dscale,
+ * dquat, ddensity, dfeatures (clipped as fast_ellipsoid_splinetracer.py:204-219). */
+int ever_scene_finalize_gradients(const EverScene* scene, const float* mean, const float* scale,
+                                  const float* quat, const void* bwd_workspace, size_t bwd_workspace_bytes,
+                                  const EverBackwardOut* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
