@@ -48,6 +48,12 @@ class EverBatch(ctypes.Structure):
                 ("bwd_workspace", c_p * 64)]
 
 
+class EverMlp(ctypes.Structure):
+    _fields_ = [("params", c_p), ("w1", c_p), ("w2", c_p), ("w3", c_p), ("centre", c_f32 * 3), ("inv_scale", c_f32)]
+
+
+MLP_PARAMS = 9360
+
 STATUS_STACK_OVERFLOW = 1
 STATUS_LOG_OVERFLOW = 2
 STATUS_INIT_OVERFLOW = 4
@@ -83,6 +89,16 @@ SIGNATURES = {
                                                    c_p, ctypes.POINTER(EverTune), c_p]),
     "ever_scene_finalize_gradients": (ctypes.c_int, [ctypes.POINTER(EverScene), c_p, c_p, c_p, c_p, c_sz,
                                                      ctypes.POINTER(EverBackwardOut), c_p]),
+    "ever_mlp_workspace_bytes": (c_sz, []),
+    "ever_mlp_pack": (ctypes.c_int, [ctypes.POINTER(EverMlp), c_p]),
+    "ever_mlp_predict": (ctypes.c_int, [ctypes.POINTER(EverMlp), c_p, c_p, c_p, c_i64, c_p, c_p,
+                                        ctypes.POINTER(c_f32), c_p, c_p]),
+    "ever_mlp_gradients": (ctypes.c_int, [ctypes.POINTER(EverMlp), c_p, c_p, c_p, c_p, c_i64, c_p, c_f32, c_f32,
+                                          c_p, c_p, c_p, c_sz, c_p, c_p]),
+    "ever_mlp_adam": (ctypes.c_int, [ctypes.POINTER(EverMlp), c_p, c_p, c_p, c_f32, c_f32, c_f32, c_f32, c_i32,
+                                     c_p]),
+    "ever_ray_order_binned": (ctypes.c_int, [c_p, c_p, c_p, c_i64, c_p, c_sz, c_p, c_p]),
+    "ever_batch_order_binned": (ctypes.c_int, [ctypes.POINTER(EverBatch), c_p, c_p, c_p, c_p]),
 }
 
 _lock = threading.Lock()

@@ -29,10 +29,12 @@ class SceneGrads:
 
 class BatchedTracer:
     def __init__(self, scenes, views, tmin=0.0, tmax=1000.0, max_iters=500, tune: T.Tune | None = None,
-                 sh_degree=None, graph=False):
+                 sh_degree=None, graph=False, scheduler=None):
         """scenes: list of (mean, scale, quat, density, features) CUDA tensors (kept by
         reference: update them in place between steps). views: list of (scene_index, rayo,
-        rayd); the rays are copied into one concatenated buffer (self.rayo / self.rayd)."""
+        rayd); the rays are copied into one concatenated buffer (self.rayo / self.rayd).
+        scheduler: optional (CostModel, thresholds): every step then predicts each ray's
+        cost bin and orders each view's rays costliest bin first."""
         if not scenes or not views:
             raise RuntimeError("a batch needs at least one scene and one view")
         self.device = scenes[0][0].device
@@ -96,8 +98,20 @@ class BatchedTracer:
             bo.dmean, bo.dscale, bo.dquat, bo.ddensity = N.ptr(g.mean), N.ptr(g.scale), N.ptr(g.quat), N.ptr(g.density)
             bo.dfeatures, bo.drayo, bo.drayd, bo.dmeans2d = N.ptr(g.features), None, None, None
             self._bo.append(bo)
+        self.scheduler = None
         self.graph = None
+        if scheduler is not None:
+            self.set_scheduler(*scheduler)
         if graph:
+            self.capture()
+
+    def set_scheduler(self, cost_model, thresholds):
+        """Uses the cost model's bins for the launch order from the next step on (a captured
+        graph is recorded again)."""
+        self.scheduler = (cost_model, [float(t) for t in thresholds])
+        self.pred = torch.empty((self.R, 2), dtype=torch.float32, device=self.device)
+        self.bins = torch.empty(self.R, dtype=torch.uint8, device=self.device)
+        if self.graph is not None:
             self.capture()
 
     def _stream(self):
@@ -108,7 +122,14 @@ class BatchedTracer:
             s.rebuild()
 
     def order(self):
-        N.check(N.load().ever_batch_order(ctypes.byref(self.batch), N.ptr(self.rayo), N.ptr(self.rayd), self._stream()))
+        lib = N.load()
+        if self.scheduler is None:
+            N.check(lib.ever_batch_order(ctypes.byref(self.batch), N.ptr(self.rayo), N.ptr(self.rayd), self._stream()))
+            return
+        cm, thr = self.scheduler
+        cm.predict(self.rayo, self.rayd, thr, out=self.pred, bins_out=self.bins)
+        N.check(lib.ever_batch_order_binned(ctypes.byref(self.batch), N.ptr(self.rayo), N.ptr(self.rayd),
+                                            N.ptr(self.bins), self._stream()))
 
     def forward(self):
         N.check(N.load().ever_trace_forward_batched(ctypes.byref(self.batch), N.ptr(self.rayo), N.ptr(self.rayd),

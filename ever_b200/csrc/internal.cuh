@@ -36,9 +36,13 @@ void sort_pairs(uint32_t*& ka, uint32_t*& va, uint32_t*& kb, uint32_t*& vb, uint
                 cudaStream_t st);
 int64_t ray_order_workspace(int64_t R);
 struct BatchView;
+// bins (nullable, one byte per ray, 0..3, larger = costlier): when given, rays of a higher
+// cost bin come first, each bin in the usual coherent order.
 cudaError_t batch_ray_order(const float* rayo, const float* rayd, int64_t R, const BatchView* views, int num_views,
-                            char* ws, int32_t* slot_ray, int64_t num_slots, cudaStream_t st);
-cudaError_t ray_order(const float* rayo, const float* rayd, int64_t R, char* ws, int32_t* order, cudaStream_t st);
+                            char* ws, int32_t* slot_ray, int64_t num_slots, cudaStream_t st,
+                            const uint8_t* bins = nullptr);
+cudaError_t ray_order(const float* rayo, const float* rayd, int64_t R, char* ws, int32_t* order, cudaStream_t st,
+                      const uint8_t* bins = nullptr);
 cudaError_t scene_build(const float* mean, const float* scale, const float* quat, const float* density,
                         const float* feat, int64_t N, int K, char* ws, const SceneLayout& L, EverScene* sc,
                         cudaStream_t st);
@@ -173,5 +177,42 @@ struct FinalizeParams {
 cudaError_t launch_finalize(const FinalizeParams& P, cudaStream_t st);
 cudaError_t launch_log_to_reference(const int32_t* order, const int32_t* log, int log_cap, const int32_t* iters,
                                     int64_t R, const int32_t* ray_order, int32_t* tri, int max_iters, cudaStream_t st);
+
+// ---- ray-cost model (39 -> 64 -> 64 -> 2 MLP on the tensor cores) ----
+// fp32 parameter block: W1 [64 x 64], W2 [64 x 64], W3 [16 x 64] (row = output unit), then
+// b1 [64], b2 [64], b3 [16]. Input columns 39..63 of W1 and output rows 2..15 of W3 pad the
+// shapes to the MMA tile and stay zero.
+constexpr int kOffW1 = 0, kOffW2 = 4096, kOffW3 = 8192, kOffB1 = 9216, kOffB2 = 9280, kOffB3 = 9344;
+constexpr int kMlpParams = 9360;
+constexpr int kMlpMaxGrid = 160;  // CTAs of a gradient launch (one partial-gradient slot each)
+
+struct MlpParams {
+  const void* w1;  // bf16 [64 x 64]
+  const void* w2;  // bf16 [64 x 64]
+  const void* w3;  // bf16 [16 x 64]
+  const float* params;
+  const float* rayo;  // rays to encode, or
+  const float* rayd;
+  const float* feat;  // pre-encoded inputs (num x 64 fp32), used instead of the rays when set
+  const int32_t* sample_idx;  // sample s reads ray sample_idx[s] (nullable: s)
+  int64_t num_samples;
+  float cx, cy, cz, inv_scale;  // scene centre and 1 / scale of the encoding
+  // inference
+  float* pred;     // (rays, 2), indexed by ray
+  uint8_t* bins;   // nullable: cost bin of each ray from pred[.,0] and the thresholds
+  float thr[3];
+  // training
+  const float* target;  // (rays, 2)
+  float loss_w0, loss_w1, inv_batch;
+  float* partial;  // (grid, kMlpParams + 1): per-CTA gradient and loss
+  int32_t* error;  // set to 1 when a tensor-core wait times out
+};
+
+cudaError_t launch_mlp(const MlpParams& P, bool train, int max_grid, cudaStream_t st);
+int mlp_grid(int64_t num_samples, int max_grid);  // CTAs launch_mlp uses
+cudaError_t launch_mlp_reduce(const float* partial, int grid, float* grads, float* loss, cudaStream_t st);
+cudaError_t launch_mlp_adam(float* params, const float* grads, float* m, float* v, void* w1, void* w2, void* w3,
+                            float lr, float beta1, float beta2, float eps, int step, cudaStream_t st);
+cudaError_t launch_mlp_pack(const float* params, void* w1, void* w2, void* w3, cudaStream_t st);
 
 }  // namespace ever

@@ -1,6 +1,6 @@
-// Coherent ray order for the packet traversal: rays are sorted by a 32-bit key made of
+// Coherent ray order for the packet traversal: rays are sorted by a 30-bit key made of
 // a coarse origin cell (6 bits) above the Morton code of the octahedral projection of
-// the direction (12 bits per axis). Thirty-two consecutive rays of the result then cover
+// the direction (12 bits per axis); a predicted cost bin, when given, goes on top. Thirty-two consecutive rays of the result then cover
 // a compact patch of directions (a screen tile for a pinhole camera), so a warp's packet
 // walks far fewer nodes than a scanline strip would. The order only decides which
 // thread picks up which ray; results do not depend on it.
@@ -19,8 +19,13 @@ __device__ __forceinline__ uint32_t spread2(uint32_t v) {  // 16 bits -> even bi
   return v;
 }
 
+// Rank of a cost bin in the sort: costlier bins (larger values) sort first.
+__device__ __forceinline__ uint32_t bin_rank(const uint8_t* __restrict__ bins, int64_t r) {
+  return 3u - min(uint32_t(bins[r]), 3u);
+}
+
 __global__ void k_ray_keys(const float* __restrict__ rayo, const float* __restrict__ rayd, int64_t R,
-                           uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+                           const uint8_t* __restrict__ bins, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
   const int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (r >= R) return;
   float dx = rayd[3 * r], dy = rayd[3 * r + 1], dz = rayd[3 * r + 2];
@@ -44,7 +49,8 @@ __global__ void k_ray_keys(const float* __restrict__ rayo, const float* __restri
     const uint32_t q = o == o ? uint32_t(fminf(fmaxf((o + 4.f) * 0.5f, 0.f), 3.f)) : 0u;  // 4 cells on [-4, 4]
     cell = (cell << 2) | q;
   }
-  keys[r] = (cell << 24) | (spread2(qu) << 1) | spread2(qv);
+  const uint32_t key = (cell << 24) | (spread2(qu) << 1) | spread2(qv);
+  keys[r] = bins ? (bin_rank(bins, r) << 30) | key : key;
   vals[r] = uint32_t(r);
 }
 
@@ -56,8 +62,10 @@ __device__ __forceinline__ int view_of(const BatchView* __restrict__ views, int 
 
 // Batched keys: the view index above the direction's Morton code, so one sort orders every
 // view at once and keeps the views apart.
+// With cost bins the bin's rank sits between the view (6 bits) and the Morton code.
 __global__ void k_batch_ray_keys(const float* __restrict__ rayd, int64_t R, const BatchView* __restrict__ views,
-                                 int num_views, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+                                 int num_views, const uint8_t* __restrict__ bins, uint32_t* __restrict__ keys,
+                                 uint32_t* __restrict__ vals) {
   const int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (r >= R) return;
   float dx = rayd[3 * r], dy = rayd[3 * r + 1], dz = rayd[3 * r + 2];
@@ -75,7 +83,8 @@ __global__ void k_batch_ray_keys(const float* __restrict__ rayd, int64_t R, cons
   }
   const uint32_t qu = min(uint32_t(fmaxf(u * 0.5f + 0.5f, 0.f) * 4096.f), 4095u);
   const uint32_t qv = min(uint32_t(fmaxf(v * 0.5f + 0.5f, 0.f) * 4096.f), 4095u);
-  keys[r] = (uint32_t(view_of(views, num_views, r)) << 24) | (spread2(qu) << 1) | spread2(qv);
+  const uint32_t view = uint32_t(view_of(views, num_views, r)), dir = (spread2(qu) << 1) | spread2(qv);
+  keys[r] = bins ? (view << 26) | (bin_rank(bins, r) << 24) | dir : (view << 24) | dir;
   vals[r] = uint32_t(r);
 }
 
@@ -91,7 +100,7 @@ __global__ void k_batch_fill_slots(const uint32_t* __restrict__ sorted, int64_t 
 }  // namespace
 
 cudaError_t batch_ray_order(const float* rayo, const float* rayd, int64_t R, const BatchView* views, int num_views,
-                            char* ws, int32_t* slot_ray, int64_t num_slots, cudaStream_t st) {
+                            char* ws, int32_t* slot_ray, int64_t num_slots, cudaStream_t st, const uint8_t* bins) {
   (void)rayo;
   cudaError_t e = cudaMemsetAsync(slot_ray, 0xff, num_slots * sizeof(int32_t), st);
   if (e != cudaSuccess || R == 0) return e;
@@ -101,8 +110,8 @@ cudaError_t batch_ray_order(const float* rayo, const float* rayd, int64_t R, con
   uint32_t* kb = reinterpret_cast<uint32_t*>(ws + c.take(R * 4));
   uint32_t* vb = reinterpret_cast<uint32_t*>(ws + c.take(R * 4));
   uint32_t* hist = reinterpret_cast<uint32_t*>(ws + c.take((int64_t(sort_blocks(R)) * 256 + 512) * 4));
-  k_batch_ray_keys<<<unsigned((R + 255) / 256), 256, 0, st>>>(rayd, R, views, num_views, ka, va);
-  sort_pairs(ka, va, kb, vb, hist, R, 30, st);
+  k_batch_ray_keys<<<unsigned((R + 255) / 256), 256, 0, st>>>(rayd, R, views, num_views, bins, ka, va);
+  sort_pairs(ka, va, kb, vb, hist, R, bins ? 32 : 30, st);
   k_batch_fill_slots<<<unsigned((R + 255) / 256), 256, 0, st>>>(va, R, views, num_views, slot_ray);
   return cudaGetLastError();
 }
@@ -117,7 +126,8 @@ int64_t ray_order_workspace(int64_t R) {
   return c.offset;
 }
 
-cudaError_t ray_order(const float* rayo, const float* rayd, int64_t R, char* ws, int32_t* order, cudaStream_t st) {
+cudaError_t ray_order(const float* rayo, const float* rayd, int64_t R, char* ws, int32_t* order, cudaStream_t st,
+                      const uint8_t* bins) {
   if (R == 0) return cudaSuccess;
   WsCursor c;
   uint32_t* ka = reinterpret_cast<uint32_t*>(ws + c.take(R * 4));
@@ -125,8 +135,8 @@ cudaError_t ray_order(const float* rayo, const float* rayd, int64_t R, char* ws,
   uint32_t* kb = reinterpret_cast<uint32_t*>(ws + c.take(R * 4));
   uint32_t* vb = reinterpret_cast<uint32_t*>(ws + c.take(R * 4));
   uint32_t* hist = reinterpret_cast<uint32_t*>(ws + c.take((int64_t(sort_blocks(R)) * 256 + 512) * 4));
-  k_ray_keys<<<unsigned((R + 255) / 256), 256, 0, st>>>(rayo, rayd, R, ka, va);
-  sort_pairs(ka, va, kb, vb, hist, R, 30, st);
+  k_ray_keys<<<unsigned((R + 255) / 256), 256, 0, st>>>(rayo, rayd, R, bins, ka, va);
+  sort_pairs(ka, va, kb, vb, hist, R, bins ? 32 : 30, st);
   return cudaMemcpyAsync(order, va, R * sizeof(int32_t), cudaMemcpyDeviceToDevice, st);
 }
 

@@ -235,6 +235,61 @@ int ever_scene_finalize_gradients(const EverScene* scene, const float* mean, con
                                   const float* quat, const void* bwd_workspace, size_t bwd_workspace_bytes,
                                   const EverBackwardOut* out, void* stream);
 
+/* ---- learned ray-cost model and cost-binned ray orders ----
+ * No counterpart in the reference. A 39 -> 64 -> 64 -> 2 ReLU MLP predicts each ray's
+ * cost [log(1 + consumed events), depth offset / scale] from a sinusoidal encoding of the
+ * point of the ray's line closest to the scene centre (x, sin(2^k pi x), cos(2^k pi x),
+ * k = 0..5). BF16 weights and activations, FP32 accumulation, tcgen05 tensor cores. It is
+ * trained on the tracer's own per-ray logs (EverForwardOut.ray_stats) and its predicted
+ * cost bins order rays: costlier bins first, each in the coherent order. Results of the
+ * trace do not depend on the order. */
+#define EVER_MLP_PARAMS 9360
+typedef struct EverMlp {
+  float* params;    /* device fp32 [EVER_MLP_PARAMS]: W1 [64x64], W2 [64x64], W3 [16x64] (row =
+                       output unit), b1 [64], b2 [64], b3 [16]; W1 columns 39..63 and W3 rows
+                       2..15 are padding and must stay zero */
+  void* w1;         /* device bf16 copies of W1, W2, W3 read by the tensor cores; refreshed */
+  void* w2;         /* by ever_mlp_pack and ever_mlp_adam */
+  void* w3;
+  float centre[3];  /* scene centre of the encoding */
+  float inv_scale;  /* 1 / scene scale of the encoding */
+} EverMlp;
+
+/* Bytes of workspace ever_mlp_gradients needs (per-CTA partial gradients). */
+size_t ever_mlp_workspace_bytes(void);
+
+/* Rounds the fp32 weights to the bf16 copies. */
+int ever_mlp_pack(const EverMlp* mlp, void* stream);
+
+/* Predictions pred (num_rays, 2) for rays (rayo, rayd) or for pre-encoded inputs feat
+ * (num_rays, 64; used when not NULL). bins (nullable): cost bin of each ray, the number of
+ * thresholds[0..2] (host array) that pred[., 0] exceeds. error: device int32 set to 1 if a
+ * tensor-core wait timed out (the outputs are then invalid). */
+int ever_mlp_predict(const EverMlp* mlp, const float* rayo, const float* rayd, const float* feat, int64_t num_rays,
+                     float* pred, uint8_t* bins, const float* thresholds, int32_t* error, void* stream);
+
+/* Gradient of the weighted squared error mean_s(w0 (y0 - t0)^2 + w1 (y1 - t1)^2) over the
+ * samples s (ray sample_idx[s], or s when sample_idx is NULL; target (rays, 2)) with respect
+ * to the fp32 parameters, written to grads [EVER_MLP_PARAMS]; the loss to *loss (nullable).
+ * Deterministic for a given device. */
+int ever_mlp_gradients(const EverMlp* mlp, const float* rayo, const float* rayd, const float* feat,
+                       const int32_t* sample_idx, int64_t num_samples, const float* target, float loss_w0,
+                       float loss_w1, float* grads, float* loss, void* workspace, size_t workspace_bytes,
+                       int32_t* error, void* stream);
+
+/* One Adam step (step counts from 1) on the fp32 parameters; refreshes the bf16 copies. */
+int ever_mlp_adam(const EverMlp* mlp, const float* grads, float* adam_m, float* adam_v, float lr, float beta1,
+                  float beta2, float eps, int32_t step, void* stream);
+
+/* ever_ray_order with cost bins (one byte per ray, 0..3, larger = costlier) on top of the
+ * key: costlier bins come first. Same workspace as ever_ray_order. */
+int ever_ray_order_binned(const float* rayo, const float* rayd, const uint8_t* bins, int64_t num_rays,
+                          void* workspace, size_t workspace_bytes, int32_t* ray_order, void* stream);
+
+/* ever_batch_order with cost bins: inside every view, costlier bins first. */
+int ever_batch_order_binned(const EverBatch* batch, const float* rayo, const float* rayd, const uint8_t* bins,
+                            void* stream);
+
 #ifdef __cplusplus
 }
 #endif
