@@ -47,6 +47,9 @@ def parse():
     p.add_argument("--verbose", action="store_true", help="per-step device times on stderr")
     p.add_argument("--once", action="store_true",
                    help="one scene build + ray order + forward + backward and exit (for ncu captures)")
+    p.add_argument("--no-batched", action="store_true", help="skip the batched multi-scene leg")
+    p.add_argument("--no-sched", action="store_true", help="skip the learned-scheduler leg")
+    p.add_argument("--sched-views", type=int, default=56, help="held-out orbit views timed in the scheduler leg")
     return p.parse_args()
 
 
@@ -200,6 +203,201 @@ def run_once(args):
                       "events_per_ray": float(fwd.iters.float().mean().item())}))
 
 
+def _timed(fn, dev):
+    """Device time (ms) of fn() with CUDA events on the current stream."""
+    import torch
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    a.record()
+    fn()
+    b.record()
+    torch.cuda.synchronize(dev)
+    return a.elapsed_time(b)
+
+
+def leg_batched(dev, reps=3):
+    """Several scenes of uneven size and views of mixed resolution: per-view launches
+    against one persistent forward + backward over all views (CUDA graph), with the
+    launch configuration the autotuner picks for the batch."""
+    import torch
+    from ever_b200 import autotune as AT
+    from ever_b200 import synthetic as S
+    from ever_b200 import tracer as T
+    from ever_b200.batched import BatchedTracer
+    scenes_np, cams = S.workload_batched(1.0)
+    scenes = [tuple(torch.tensor(np.ascontiguousarray(a), device=dev) for a in
+                    (sc.mean, sc.scale, sc.quat, sc.density.reshape(-1), sc.features)) for sc in scenes_np]
+    views = [(si, *S.look_at_rays_device(cam, dev)) for si, cam in cams]
+    R = sum(v[1].shape[0] for v in views)
+    gouts = [torch.full((v[1].shape[0], 5), 0.1, device=dev) for v in views]
+    gout = torch.cat(gouts)
+
+    def sequential(tune):
+        built = [T.Scene(*sc) for sc in scenes]
+        for (si, ro, rd), g in zip(views, gouts):
+            order = T.ray_order(ro, rd)
+            f = T.forward(built[si], ro, rd, 0.0, 1000.0, 500, ray_order=order, tune=tune)
+            T.backward(built[si], ro, rd, f, g, 0.0, 1000.0, 500, ray_order=order, tune=tune)
+
+    bt = BatchedTracer(scenes, views, max_iters=500, graph=False)
+
+    def run_cand(c):
+        bt.tune = c.tune()
+        bt.step(gout)
+        return int(bt.status.item())
+
+    best, timings = AT.autotune(run_cand, AT.workload_key(sum(int(s[0].shape[0]) for s in scenes), R, 16, dev),
+                                candidates=[c for c in AT.DEFAULT_CANDIDATES if c.ordered], warmup=1, reps=1,
+                                force=True)
+    tune = best.tune()
+    bt = BatchedTracer(scenes, views, max_iters=500, tune=tune, graph=True)
+    bt.step(gout)
+    sequential(tune)
+    seq = float(np.median([_timed(lambda: sequential(tune), dev) for _ in range(reps)]))
+    bat = float(np.median([_timed(lambda: bt.step(gout), dev) for _ in range(reps)]))
+    ok = int(bt.status.item()) == 0
+    del bt
+    torch.cuda.empty_cache()
+    return {"workload": "3 clustered scenes (50k, 500k, 2M ellipsoids, SH3), 16 views from 320x240 to 1920x1080, "
+                        "forward + backward, BVH rebuilt per step",
+            "rays": R, "sequential_ms": seq, "batched_graph_ms": bat,
+            "sequential_mrays": R / (seq * 1e-3) / 1e6, "batched_mrays": R / (bat * 1e-3) / 1e6,
+            "speedup_batched_vs_sequential": seq / bat, "autotuned": {"kbuf": best.kbuf, "block": best.block,
+                                                                       "traversal": best.traversal},
+            "status_clean": ok}
+
+
+def leg_sched(dev, test_views=56):
+    """Learned ray-cost scheduler on a 64-view orbit of 3M clustered ellipsoids: the MLP is
+    trained on the first 8 views' per-ray logs, then the remaining views are traced forward
+    + backward in plain order, coherent order, learned cost-binned order (MLP inference and
+    sort inside the timed region), the learned order in batched persistent launches of 8
+    views, and cost bins from the true logged costs (a ceiling no predictor can beat)."""
+    import torch
+    from ever_b200 import scheduler as SCH
+    from ever_b200 import synthetic as S
+    from ever_b200 import tracer as T
+    from ever_b200.batched import BatchedTracer
+    n_train, W, H = 8, 1920, 1080
+    sc, cams = S.workload_orbit(n=3_000_000, n_views=64, width=W, height=H)
+    arrs = tuple(torch.tensor(np.ascontiguousarray(a), device=dev) for a in
+                 (sc.mean, sc.scale, sc.quat, sc.density.reshape(-1), sc.features))
+    del sc
+    scene = T.Scene(*arrs)
+    test_views = max(1, min(test_views, 64 - n_train))
+    rays = [S.look_at_rays_device(c, dev) for c in cams[:n_train + test_views]]
+    R = rays[0][0].shape[0]
+    ws = torch.empty(int(T.N.load().ever_ray_order_workspace_bytes(R)), dtype=torch.uint8, device=dev)
+    stats = []
+    for ro, rd in rays:
+        f = T.forward(scene, ro, rd, 0.0, 1000.0, 500, log_events=False, ray_stats=True,
+                      ray_order=T.ray_order(ro, rd, ws))
+        stats.append(f.ray_stats.clone())
+    ro_tr = torch.cat([r[0] for r in rays[:n_train]])
+    rd_tr = torch.cat([r[1] for r in rays[:n_train]])
+    st_tr = torch.cat(stats[:n_train])
+    cm = SCH.CostModel(scale=2.0, seed=1, device=dev)
+    tg = SCH.cost_targets(st_tr, ro_tr, rd_tr, scale=2.0)
+    losses = []
+    fit_ms = _timed(lambda: losses.append(cm.fit(ro_tr, rd_tr, tg, epochs=3, batch=65536, lr=3e-3)), dev)
+    cm.check()
+    losses = losses[0].cpu().numpy()
+    thr = SCH.quantile_thresholds(cm.predict(ro_tr, rd_tr)[0][:, 0])
+    true_thr = SCH.quantile_thresholds(torch.log1p(st_tr[:, 0]))
+    del ro_tr, rd_tr, st_tr, tg
+    test = list(range(n_train, n_train + test_views))
+    pred_buf = torch.empty((R, 2), device=dev)
+    bins_buf = torch.empty(R, dtype=torch.uint8, device=dev)
+    order_buf = torch.empty(R, dtype=torch.int32, device=dev)
+    predict_ms = _timed(lambda: cm.predict(*rays[test[0]], thresholds=thr, out=pred_buf, bins_out=bins_buf), dev)
+    r2 = []
+    true_bins = {}
+    for v in test:
+        p, _ = cm.predict(*rays[v])
+        t = torch.log1p(stats[v][:, 0])
+        r2.append(1 - float(((p[:, 0] - t) ** 2).mean() / t.var()))
+        true_bins[v] = ((t > true_thr[0]).int() + (t > true_thr[1]).int() + (t > true_thr[2]).int()).to(torch.uint8)
+    del stats
+    gout = torch.full((R, 5), 0.1, device=dev)
+    fbuf = [None]
+    bws = [None]
+    outs = {}
+
+    def order_of(kind, v):
+        ro, rd = rays[v]
+        if kind == "plain":
+            return None
+        if kind == "coherent":
+            return T.ray_order(ro, rd, ws)
+        if kind == "learned":
+            cm.predict(ro, rd, thresholds=thr, out=pred_buf, bins_out=bins_buf)
+            return SCH.binned_order(ro, rd, bins_buf, ws, order_buf)
+        return SCH.binned_order(ro, rd, true_bins[v], ws, order_buf)
+
+    def one(kind, v):
+        ro, rd = rays[v]
+        o = order_of(kind, v)
+        f = T.forward(scene, ro, rd, 0.0, 1000.0, 500, ray_order=o, buffers=fbuf[0])
+        fbuf[0] = f
+        g = T.backward(scene, ro, rd, f, gout, 0.0, 1000.0, 500, ray_order=o, workspace=bws[0])
+        return f, g
+
+    one("plain", test[0])
+    bws[0] = torch.empty(int(T.N.load().ever_backward_workspace_bytes(scene.num_prims, scene.sh_coeffs)),
+                         dtype=torch.uint8, device=dev)
+    ms = {}
+    identical = True
+    for kind in ("plain", "coherent", "learned", "true"):
+        one(kind, test[0])
+        ms[kind] = _timed(lambda: [one(kind, v) for v in test], dev)
+        for v in test:  # images of every order against the plain order's
+            f, _ = one(kind, v)
+            if kind == "plain":
+                outs[v] = f.out.clone()
+            else:
+                identical &= bool(torch.equal(f.out, outs[v]))
+    del fbuf[0], bws[0]
+    torch.cuda.empty_cache()
+    # learned order in batched persistent launches (8 views per launch; graph capture)
+    batched_ms = 0.0
+    for i in range(0, len(test), 8):
+        grp = test[i:i + 8]
+        bt = BatchedTracer([arrs], [(0, *rays[v]) for v in grp], max_iters=500, graph=True, scheduler=(cm, thr))
+        g = torch.full((bt.R, 5), 0.1, device=dev)
+        batched_ms += _timed(lambda: bt.step(g), dev)
+        for j, v in enumerate(grp):
+            identical &= bool(torch.equal(bt.out[bt.view_slice(j)], outs[v]))
+        del bt, g
+        torch.cuda.empty_cache()
+    rays_total = R * len(test)
+    mr = lambda t: rays_total / (t * 1e-3) / 1e6
+    flop_per_ray = 2 * (39 * 64 + 64 * 64 + 64 * 2)
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            bf16_peak, peak_kind = float(json.load(fh)["bf16_tflops"]), "measured"
+    except Exception:
+        bf16_peak, peak_kind = 1590.0, "fallback"
+    mlp_tflops = R * flop_per_ray / (predict_ms * 1e-3) / 1e12
+    return {
+        "workload": f"3M clustered ellipsoids SH3, 64-view orbit at radius 4, {W}x{H}; MLP trained on views 0-7, "
+                    f"views 8-{7 + test_views} traced forward + backward",
+        "mrays_fwdbwd": {"plain": mr(ms["plain"]), "coherent": mr(ms["coherent"]), "learned": mr(ms["learned"]),
+                         "learned_batched": mr(batched_ms), "true_cost_bins": mr(ms["true"])},
+        "ms_total": dict(ms, learned_batched=batched_ms),
+        "speedup_learned_vs_plain": ms["plain"] / ms["learned"],
+        "speedup_learned_batched_vs_plain": ms["plain"] / batched_ms,
+        "speedup_learned_vs_coherent": ms["coherent"] / ms["learned"],
+        "speedup_true_cost_bins_vs_coherent": ms["coherent"] / ms["true"],
+        "images_bit_identical_to_plain": identical,
+        "heldout_r2_log_events_mean": float(np.mean(r2)),
+        "train": {"samples": R * n_train, "steps": int(len(losses)), "fit_ms": fit_ms,
+                  "loss_first": float(losses[0]), "loss_last": float(losses[-1])},
+        "mlp_predict": {"ms_per_view": predict_ms, "rays": R, "tflops": mlp_tflops, "peak_tflops": bf16_peak,
+                        "frac": mlp_tflops / bf16_peak, "peak_kind": peak_kind,
+                        "flop_per_ray": flop_per_ray},
+    }
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -282,9 +480,9 @@ def main():
     # ---- phase breakdown (outside the timed region): build / forward / backward kernels
     def phases(reps=3):
         scene_t = [params[k].detach() for k in ("mean", "scale", "quat", "density", "features")]
-        res = {"order": [], "build": [], "fwd": [], "bwd": []}
+        res = {"order": [], "build": [], "fwd": [], "bwd_order": [], "bwd": []}
         for _ in range(reps):
-            e = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
             e[0].record()
             order = T.ray_order(rayo, rayd)
             e[1].record()
@@ -292,13 +490,16 @@ def main():
             e[2].record()
             fwd = T.forward(scene, rayo, rayd, 0.0, 1000.0, 500, tune=tune, ray_stats=True, ray_order=order)
             e[3].record()
-            T.backward(scene, rayo, rayd, fwd, gout, 0.0, 1000.0, 500, tune=tune, ray_order=order)
+            slots = T.backward_order(fwd, order, 0)
             e[4].record()
+            T.backward(scene, rayo, rayd, fwd, gout, 0.0, 1000.0, 500, tune=tune, ray_order=order, slot_order=slots)
+            e[5].record()
             torch.cuda.synchronize()
             res["order"].append(e[0].elapsed_time(e[1]))
             res["build"].append(e[1].elapsed_time(e[2]))
             res["fwd"].append(e[2].elapsed_time(e[3]))
-            res["bwd"].append(e[3].elapsed_time(e[4]))
+            res["bwd_order"].append(e[3].elapsed_time(e[4]))
+            res["bwd"].append(e[4].elapsed_time(e[5]))
         med = {k: float(np.median(v)) for k, v in res.items()}
         stats = fwd.ray_stats
         med["events_per_ray"] = float(stats[:, 0].mean().item())
@@ -361,11 +562,12 @@ def main():
         "fwd_mrays_trace_only": R / (ph["fwd"] * 1e-3) / 1e6,
         "fwd_mrays_with_build": R / ((ph["fwd"] + ph["build"] + ph["order"]) * 1e-3) / 1e6,
         "fwdbwd_mrays_trace_only": R / ((ph["fwd"] + ph["bwd"]) * 1e-3) / 1e6,
-        "fwdbwd_mrays_with_build": R / ((ph["fwd"] + ph["bwd"] + ph["build"] + ph["order"]) * 1e-3) / 1e6,
+        "fwdbwd_mrays_with_build": R / ((ph["fwd"] + ph["bwd"] + ph["build"] + ph["order"] + ph["bwd_order"]) * 1e-3)
+        / 1e6,
         "phase_ms": ph,
         "clocks": clk.summary(),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": args.steps * 20,
+        "gpu_launches": args.steps * 57,
         "roofline": roofline,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -373,6 +575,11 @@ def main():
         v, dt, n = cpu_baseline(sc, ro, rd, threads, target_s=10.0, n_rays=args.cpu_sample)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"{n} seeded rays of the view, forward + FP64 backward, {dt:.1f} s"}
+    if rank == 0 and world == 1 and not args.no_batched:
+        line["batched"] = leg_batched(dev)
+    if rank == 0 and world == 1 and not args.no_sched:
+        line["sched"] = leg_sched(dev, args.sched_views)
+        line["learned_sched_vs_plain_speedup"] = line["sched"]["speedup_learned_vs_plain"]
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

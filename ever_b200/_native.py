@@ -72,6 +72,11 @@ SIGNATURES = {
     "ever_trace_backward": (ctypes.c_int, [ctypes.POINTER(EverScene), c_p, c_p, c_i64, ctypes.POINTER(EverTraceArgs),
                                            c_p, c_p, c_p, c_p, c_i32, c_p, c_i32, c_p, c_p, c_p, c_p, c_sz, c_p,
                                            ctypes.POINTER(EverTune), ctypes.POINTER(EverBackwardOut), c_p]),
+    "ever_trace_backward_ordered": (ctypes.c_int, [ctypes.POINTER(EverScene), c_p, c_p, c_i64,
+                                                   ctypes.POINTER(EverTraceArgs), c_p, c_p, c_p, c_p, c_i32, c_p,
+                                                   c_i32, c_p, c_p, c_p, c_p, c_sz, c_p, c_p,
+                                                   ctypes.POINTER(EverTune), ctypes.POINTER(EverBackwardOut), c_p]),
+    "ever_backward_slot_order": (ctypes.c_int, [c_p, c_p, c_i64, c_i32, c_p, c_sz, c_p, c_p]),
     "ever_event_log_to_reference": (ctypes.c_int, [ctypes.POINTER(EverScene), c_p, c_i32, c_p, c_i64, c_p, c_p,
                                                    c_i32, c_p]),
     "ever_ray_order_workspace_bytes": (c_sz, [c_i64]),

@@ -126,12 +126,16 @@ size_t ever_backward_workspace_bytes(int64_t num_prims, int32_t sh_coeffs) {
   return size_t(c.offset);
 }
 
-int ever_trace_backward(const EverScene* scene, const float* rayo, const float* rayd, int64_t num_rays,
-                        const EverTraceArgs* args, const float* grad_out, const float* states,
-                        const int32_t* iters, const int32_t* event_log, int32_t log_cap, const float* wct,
-                        int32_t num_wct, const float* mean, const float* scale, const float* quat, void* workspace,
-                        size_t workspace_bytes, const int32_t* ray_order, const EverTune* tune,
-                        const EverBackwardOut* out, void* stream) {
+}  // extern "C"
+
+namespace {
+
+int trace_backward(const EverScene* scene, const float* rayo, const float* rayd, int64_t num_rays,
+                   const EverTraceArgs* args, const float* grad_out, const float* states, const int32_t* iters,
+                   const int32_t* event_log, int32_t log_cap, const float* wct, int32_t num_wct, const float* mean,
+                   const float* scale, const float* quat, void* workspace, size_t workspace_bytes,
+                   const int32_t* ray_order, const int32_t* slot_order, const EverTune* tune,
+                   const EverBackwardOut* out, void* stream) {
   if (!scene || !args || !out) return fail(EVER_ERR_INVALID, "null scene, args or out");
   const int64_t N = scene->num_prims;
   if (num_rays < 0) return fail(EVER_ERR_INVALID, "num_rays out of range");
@@ -178,6 +182,7 @@ int ever_trace_backward(const EverScene* scene, const float* rayo, const float* 
     P.tmax = args->tmax;
     P.max_iters = args->max_iters;
     P.ray_order = ray_order;
+    P.slot_order = slot_order;
     P.grad_out = grad_out;
     P.states = states;
     P.iters = iters;
@@ -214,6 +219,46 @@ int ever_trace_backward(const EverScene* scene, const float* rayo, const float* 
     if (e == cudaSuccess) e = cudaMemsetAsync(out->drayd, 0, num_rays * 3 * sizeof(float), st);
   }
   return cuda_status(e, "ever_trace_backward");
+}
+
+}  // namespace
+
+extern "C" {
+
+int ever_trace_backward(const EverScene* scene, const float* rayo, const float* rayd, int64_t num_rays,
+                        const EverTraceArgs* args, const float* grad_out, const float* states,
+                        const int32_t* iters, const int32_t* event_log, int32_t log_cap, const float* wct,
+                        int32_t num_wct, const float* mean, const float* scale, const float* quat, void* workspace,
+                        size_t workspace_bytes, const int32_t* ray_order, const EverTune* tune,
+                        const EverBackwardOut* out, void* stream) {
+  return trace_backward(scene, rayo, rayd, num_rays, args, grad_out, states, iters, event_log, log_cap, wct, num_wct,
+                        mean, scale, quat, workspace, workspace_bytes, ray_order, nullptr, tune, out, stream);
+}
+
+int ever_trace_backward_ordered(const EverScene* scene, const float* rayo, const float* rayd, int64_t num_rays,
+                                const EverTraceArgs* args, const float* grad_out, const float* states,
+                                const int32_t* iters, const int32_t* event_log, int32_t log_cap, const float* wct,
+                                int32_t num_wct, const float* mean, const float* scale, const float* quat,
+                                void* workspace, size_t workspace_bytes, const int32_t* ray_order,
+                                const int32_t* slot_order, const EverTune* tune, const EverBackwardOut* out,
+                                void* stream) {
+  if (num_rays > 0 && !slot_order) return fail(EVER_ERR_INVALID, "ever_trace_backward_ordered: null slot_order");
+  return trace_backward(scene, rayo, rayd, num_rays, args, grad_out, states, iters, event_log, log_cap, wct, num_wct,
+                        mean, scale, quat, workspace, workspace_bytes, ray_order, slot_order, tune, out, stream);
+}
+
+int ever_backward_slot_order(const int32_t* iters, const int32_t* ray_order, int64_t num_rays, int32_t shift,
+                             void* workspace, size_t workspace_bytes, int32_t* slot_order, void* stream) {
+  if (num_rays < 0 || num_rays >= (int64_t(1) << 31)) return fail(EVER_ERR_INVALID, "num_rays out of range");
+  if (shift < 0 || shift > 16) return fail(EVER_ERR_INVALID, "shift %d out of range 0..16", shift);
+  if (num_rays > 0 && (!iters || !slot_order)) return fail(EVER_ERR_INVALID, "null pointer");
+  const int64_t need = ever::ray_order_workspace(num_rays);
+  if (num_rays > 0 && (!workspace || workspace_bytes < size_t(need)))
+    return fail(EVER_ERR_WORKSPACE, "slot order workspace needs %lld bytes, got %zu", (long long)need,
+                workspace_bytes);
+  return cuda_status(ever::backward_slot_order(iters, ray_order, num_rays, shift, static_cast<char*>(workspace),
+                                               slot_order, static_cast<cudaStream_t>(stream)),
+                     "ever_backward_slot_order");
 }
 
 int ever_event_log_to_reference(const EverScene* scene, const int32_t* event_log, int32_t log_cap,

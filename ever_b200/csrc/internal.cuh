@@ -43,6 +43,11 @@ cudaError_t batch_ray_order(const float* rayo, const float* rayd, int64_t R, con
                             const uint8_t* bins = nullptr);
 cudaError_t ray_order(const float* rayo, const float* rayd, int64_t R, char* ws, int32_t* order, cudaStream_t st,
                       const uint8_t* bins = nullptr);
+// Backward launch order over forward slots: slots whose rays consumed more events first
+// (key min(iters >> shift, 255), descending), the forward's slot order inside a key.
+// Workspace: ray_order_workspace(R).
+cudaError_t backward_slot_order(const int32_t* iters, const int32_t* ray_order, int64_t R, int shift, char* ws,
+                                int32_t* slot_order, cudaStream_t st);
 cudaError_t scene_build(const float* mean, const float* scale, const float* quat, const float* density,
                         const float* feat, int64_t N, int K, char* ws, const SceneLayout& L, EverScene* sc,
                         cudaStream_t st);
@@ -143,6 +148,7 @@ struct BwdParams {
   float tmin, tmax;
   int max_iters;
   const int32_t* ray_order;
+  const int32_t* slot_order;  // nullable: launch position -> forward slot
   const float* grad_out;
   const float* states;
   const int32_t* iters;

@@ -488,12 +488,13 @@ __global__ void __launch_bounds__(256) k_trace_bwd(const BwdParams P) {
   const int tid = threadIdx.x;
   const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;
   if (gi >= P.R) return;
-  const int64_t r = P.ray_order ? int64_t(P.ray_order[gi]) : gi;
+  const int64_t slot = P.slot_order ? int64_t(P.slot_order[gi]) : gi;  // event-log column
+  const int64_t r = P.ray_order ? int64_t(P.ray_order[slot]) : slot;
   const BScene S{reinterpret_cast<const Node*>(P.nodes), reinterpret_cast<const Record*>(P.records), P.features, P.K,
                  P.acc_geo, P.acc_feat};
   const BRayCtx C{P.rayo, P.rayd, P.tmin, P.max_iters, P.grad_out, P.states, P.iters, P.event_log, P.R,
                   P.drayo, P.drayd, P.wct, P.num_wct, P.dmeans2d};
-  backward_ray<DEG>(S, C, r, gi, smem + tid, blockDim.x);
+  backward_ray<DEG>(S, C, r, slot, smem + tid, blockDim.x);
 }
 
 // Persistent batched backward: warps take 32-slot packets from a device counter.

@@ -108,8 +108,12 @@ class SplineTracer(Function):
     @staticmethod
     def backward(ctx, grad_output: torch.Tensor, *unused):
         rayo, rayd, wcts = ctx.saved_tensors
+        # replay order: rays grouped by the number of events the forward consumed (longest
+        # first), so a warp's 32 reverse replays run for the same number of steps
+        slot_order = T.backward_order(ctx.fwd, ctx.ray_order, 0) if rayo.shape[0] > 0 else None
         g = T.backward(ctx.scene, rayo, rayd, ctx.fwd, grad_output, ctx.tmin, ctx.tmax, ctx.max_iters,
-                       ctx.sh_degree, wcts=wcts, want_means2d=ctx.has_wcts, ray_order=ctx.ray_order, tune=ctx.tune)
+                       ctx.sh_degree, wcts=wcts, want_means2d=ctx.has_wcts, ray_order=ctx.ray_order, tune=ctx.tune,
+                       slot_order=slot_order)
         # the event log and scene workspace are not needed again: give them back to the allocator
         ctx.fwd = None
         ctx.scene = None

@@ -102,6 +102,28 @@ def look_at_rays(cam: Camera):
     return np.ascontiguousarray(o, np.float32), np.ascontiguousarray(d, np.float32)
 
 
+def look_at_rays_device(cam: Camera, device):
+    """look_at_rays computed with torch on `device` (float64, then float32): same rays up to
+    the last float32 bit, without the host round trip for large views."""
+    import torch
+    eye = torch.tensor(np.asarray(cam.eye, np.float64), device=device)
+    fwd = -eye / eye.norm()
+    up = torch.tensor([0.0, 0.0, 1.0] if abs(float(fwd[2])) < 0.99 else [0.0, 1.0, 0.0], dtype=torch.float64,
+                      device=device)
+    right = torch.linalg.cross(fwd, up)
+    right = right / right.norm()
+    upv = torch.linalg.cross(right, fwd)
+    f = 0.5 * cam.height / np.tan(0.5 * np.deg2rad(cam.fov_y_deg))
+    i, j = torch.meshgrid(torch.arange(cam.height, dtype=torch.float64, device=device) + 0.5,
+                          torch.arange(cam.width, dtype=torch.float64, device=device) + 0.5, indexing="ij")
+    x = ((j - 0.5 * cam.width) / f).reshape(-1, 1)
+    y = ((i - 0.5 * cam.height) / f).reshape(-1, 1)
+    d = fwd[None] + x * right[None] - y * upv[None]
+    d = d / d.norm(dim=1, keepdim=True)
+    o = eye[None].expand_as(d)
+    return o.float().contiguous(), d.float().contiguous()
+
+
 def sphere_point(radius, seed):
     rng = np.random.default_rng(seed)
     v = rng.standard_normal(3)

@@ -174,7 +174,8 @@ class Gradients:
 
 def backward(scene: Scene, rayo, rayd, fwd: ForwardResult, grad_out, tmin=0.0, tmax=1000.0, max_iters=500,
              sh_degree=None, wcts=None, want_means2d=False, ray_order=None, tune: Tune | None = None,
-             workspace: torch.Tensor | None = None) -> Gradients:
+             workspace: torch.Tensor | None = None, slot_order=None) -> Gradients:
+    """slot_order: optional launch order over the forward's slots (backward_order())."""
     device = scene.device
     if fwd.event_log is None:
         raise RuntimeError("backward needs the forward's event log (log_events=True)")
@@ -201,13 +202,35 @@ def backward(scene: Scene, rayo, rayd, fwd: ForwardResult, grad_out, tmin=0.0, t
     o.dmean, o.dscale, o.dquat, o.ddensity = N.ptr(g.mean), N.ptr(g.scale), N.ptr(g.quat), N.ptr(g.density)
     o.dfeatures, o.drayo, o.drayd, o.dmeans2d = N.ptr(g.features), N.ptr(g.rayo), N.ptr(g.rayd), N.ptr(g.means2d)
     args = trace_args(tmin, tmax, max_iters, sh_degree)
+    common = (ctypes.byref(scene.c), N.ptr(rayo), N.ptr(rayd), R, ctypes.byref(args), N.ptr(grad_out),
+              N.ptr(fwd.states), N.ptr(fwd.iters), N.ptr(fwd.event_log), fwd.event_log.shape[0], N.ptr(wct), num_wct,
+              N.ptr(m), N.ptr(s), N.ptr(q), N.ptr(workspace), int(workspace.numel()), N.ptr(ray_order))
     with torch.cuda.device(device):
-        N.check(lib.ever_trace_backward(
-            ctypes.byref(scene.c), N.ptr(rayo), N.ptr(rayd), R, ctypes.byref(args), N.ptr(grad_out),
-            N.ptr(fwd.states), N.ptr(fwd.iters), N.ptr(fwd.event_log), fwd.event_log.shape[0], N.ptr(wct), num_wct,
-            N.ptr(m), N.ptr(s), N.ptr(q), N.ptr(workspace), int(workspace.numel()), N.ptr(ray_order),
-            ctypes.byref((tune or Tune()).c()), ctypes.byref(o), _stream(device)))
+        if slot_order is None:
+            N.check(lib.ever_trace_backward(*common, ctypes.byref((tune or Tune()).c()), ctypes.byref(o),
+                                            _stream(device)))
+        else:
+            _check_tensor("slot_order", slot_order, device, None, torch.int32)
+            N.check(lib.ever_trace_backward_ordered(*common, N.ptr(slot_order), ctypes.byref((tune or Tune()).c()),
+                                                    ctypes.byref(o), _stream(device)))
     return g
+
+
+def backward_order(fwd: ForwardResult, ray_order=None, shift: int = 1,
+                   workspace: torch.Tensor | None = None) -> torch.Tensor:
+    """Backward launch order over the forward's slots: rays that consumed more events first,
+    grouped by iters >> shift, coherent slot order within a group."""
+    R = fwd.iters.numel()
+    device = fwd.iters.device
+    order = torch.empty(R, dtype=torch.int32, device=device)
+    lib = N.load()
+    need = int(lib.ever_ray_order_workspace_bytes(R))
+    if workspace is None or workspace.numel() < need:
+        workspace = torch.empty(max(need, 256), dtype=torch.uint8, device=device)
+    with torch.cuda.device(device):
+        N.check(lib.ever_backward_slot_order(N.ptr(fwd.iters), N.ptr(ray_order), R, int(shift), N.ptr(workspace),
+                                             int(workspace.numel()), N.ptr(order), _stream(device)))
+    return order
 
 
 def ray_order(rayo, rayd, workspace: torch.Tensor | None = None) -> torch.Tensor:

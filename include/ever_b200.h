@@ -140,6 +140,26 @@ int ever_trace_backward(const EverScene* scene, const float* rayo, const float* 
                         const int32_t* ray_order, const EverTune* tune, const EverBackwardOut* out,
                         void* stream);
 
+/* ever_trace_backward with its own launch order: launch position p replays forward slot
+ * slot_order[p] (a permutation of 0..R-1; the event-log column), ray ray_order[slot].
+ * The results do not depend on the order (up to the summation order of the
+ * ellipsoid gradients). No counterpart in the reference. */
+int ever_trace_backward_ordered(const EverScene* scene, const float* rayo, const float* rayd, int64_t num_rays,
+                                const EverTraceArgs* args, const float* grad_out, const float* states,
+                                const int32_t* iters, const int32_t* event_log, int32_t log_cap, const float* wct,
+                                int32_t num_wct, const float* mean, const float* scale, const float* quat,
+                                void* workspace, size_t workspace_bytes, const int32_t* ray_order,
+                                const int32_t* slot_order, const EverTune* tune, const EverBackwardOut* out,
+                                void* stream);
+
+/* A backward launch order from the forward's per-ray event counts (iters, indexed by
+ * ray; ray_order: the forward's order, nullable): slots whose rays consumed more events
+ * come first, grouped by min(iters >> shift, 255), the forward's coherent slot order
+ * inside a group. Warps then replay rays of equal length. Same workspace as
+ * ever_ray_order. No counterpart in the reference. */
+int ever_backward_slot_order(const int32_t* iters, const int32_t* ray_order, int64_t num_rays, int32_t shift,
+                             void* workspace, size_t workspace_bytes, int32_t* slot_order, void* stream);
+
 /* Converts an event log in Morton numbering into the reference's tri_collection ids
  * (2p+1 entry, 2p exit with original indices p; fast_ellipsoid_splinetracer.py:93-101),
  * (max_iters, R) indexed by ray. ray_order: the order the forward was launched with.

@@ -159,3 +159,29 @@ def test_truncated_rays_get_no_gradient():
     ref = _oracle_grads(sc, ro, rd, dout, max_iters=3, mode="f32_replay")
     for k in ref:
         assert _rel_err(g[k], _clip(k, ref[k])) < REPLAY_TOL, k
+
+
+@pytest.mark.parametrize("shift", [0, 2])
+def test_backward_slot_order_groups_rays_by_length_and_changes_no_result(shift):
+    from ever_b200 import tracer as T
+    dev = _dev()
+    sc = S.clustered_scene(20_000, 2, seed=21, n_clusters=60)
+    ro, rd = S.look_at_rays(S.Camera(S.sphere_point(4.0, 21), 48, 40, 50.0))
+    t = lambda a: torch.tensor(np.ascontiguousarray(a, np.float32), device=dev)
+    scene = T.Scene(t(sc.mean), t(sc.scale), t(sc.quat), t(sc.density.reshape(-1)), t(sc.features))
+    rayo, rayd = t(ro), t(rd)
+    order = T.ray_order(rayo, rayd)
+    fwd = T.forward(scene, rayo, rayd, ray_order=order)
+    gout = torch.randn((rayo.shape[0], 5), device=dev, generator=torch.Generator(device=dev).manual_seed(1))
+    slots = T.backward_order(fwd, order, shift)
+    R = rayo.shape[0]
+    assert torch.equal(torch.sort(slots).values, torch.arange(R, device=dev, dtype=torch.int32))
+    n = (fwd.iters[order.long()[slots.long()]] >> shift).clamp(max=255)
+    assert bool((n[1:] <= n[:-1]).all())  # longest replays first
+    same = n[1:] == n[:-1]
+    assert bool((slots[1:][same] > slots[:-1][same]).all())  # coherent slot order inside a group
+    a = T.backward(scene, rayo, rayd, fwd, gout, ray_order=order)
+    b = T.backward(scene, rayo, rayd, fwd, gout, ray_order=order, slot_order=slots)
+    assert torch.equal(a.rayo, b.rayo) and torch.equal(a.rayd, b.rayd)  # per-ray results: identical
+    for x, y in zip((a.mean, a.scale, a.quat, a.density, a.features), (b.mean, b.scale, b.quat, b.density, b.features)):
+        assert float((x - y).abs().max()) <= 1e-4 * float(y.abs().max()) + 1e-12  # summation order only

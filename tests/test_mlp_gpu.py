@@ -245,3 +245,28 @@ def test_cost_binned_orders_keep_images_bit_identical_and_balance_packets():
         print("lane slots per useful step:", s)
         assert s["true"] < s["coherent"] < s["plain"]
         assert s["learned"] < s["plain"] and s["learned"] < 1.05 * s["coherent"]
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_batched_tracer_with_learned_scheduler_matches_unscheduled(graph):
+    from ever_b200.batched import BatchedTracer
+    dev = _dev()
+    sc = S.clustered_scene(20_000, 1, seed=13, n_clusters=100)
+    arrs = tuple(torch.tensor(np.ascontiguousarray(a), device=dev) for a in
+                 (sc.mean, sc.scale, sc.quat, sc.density.reshape(-1), sc.features))
+    views = [(0, *S.look_at_rays_device(S.Camera(e, w, h, 50.0), dev))
+             for e, (w, h) in zip(S.orbit(4.0, 3), [(64, 48), (40, 30), (33, 17)])]
+    cm = SCH.CostModel(scale=2.0, seed=3, device=dev)
+    plain = BatchedTracer([arrs], views, graph=False)
+    sched = BatchedTracer([arrs], views, graph=graph, scheduler=(cm, [2.0, 2.5, 3.0]))
+    g = torch.full((plain.R, 5), 0.1, device=dev)
+    plain.step(g)
+    sched.step(g)
+    torch.cuda.synchronize()
+    assert torch.equal(plain.out, sched.out) and torch.equal(plain.iters, sched.iters)
+    assert torch.equal(plain.drayo, sched.drayo) and torch.equal(plain.drayd, sched.drayd)
+    for a, b in zip(plain.grads, sched.grads):
+        for x, y in zip([a.mean, a.density, a.features], [b.mean, b.density, b.features]):
+            assert float((x - y).abs().max()) <= 1e-4 * float(y.abs().max()) + 1e-12
+    assert int(sched.bins.max()) <= 3
+    cm.check()
