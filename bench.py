@@ -339,7 +339,8 @@ def leg_sched(dev, test_views=56):
         o = order_of(kind, v)
         f = T.forward(scene, ro, rd, 0.0, 1000.0, 500, ray_order=o, buffers=fbuf[0])
         fbuf[0] = f
-        g = T.backward(scene, ro, rd, f, gout, 0.0, 1000.0, 500, ray_order=o, workspace=bws[0])
+        slots = T.backward_order(f, o, 0, ws)  # as trace_rays' backward: replay grouped by event count
+        g = T.backward(scene, ro, rd, f, gout, 0.0, 1000.0, 500, ray_order=o, workspace=bws[0], slot_order=slots)
         return f, g
 
     one("plain", test[0])

@@ -29,7 +29,9 @@ BatchLayout batch_layout(int num_scenes, const EverBatchView* views, int num_vie
   L.view_table = c.take(int64_t(num_views) * sizeof(BatchView));
   L.slot_ray = c.take(slots * sizeof(int32_t));
   L.counters = c.take(4 * sizeof(uint32_t));
-  L.order_scratch = c.take(ray_order_workspace(std::max<int64_t>(rays, 1)));
+  // sort scratch for the ray order (rays) and the backward's slot order (slots), followed
+  // by the backward's slot order itself
+  L.order_scratch = c.take(ray_order_workspace(std::max<int64_t>(slots, 1)) + std::max<int64_t>(slots, 1) * 4);
   L.total = c.offset;
   L.num_slots = slots;
   return L;
@@ -50,12 +52,13 @@ EverTune tune_of(const EverTune* t) {
   return r;
 }
 
-// Persistent grid: enough resident blocks to fill every SM (occupancy of the kernel is
-// bounded by registers: about 16 warps per SM for the trace kernels).
-int persistent_grid(int block) {
+// Persistent grid: enough resident blocks to fill every SM. Occupancy is bounded by
+// registers: 20 warps per SM for the forward with blocks of 64 or 128 threads, 16 warps
+// otherwise (the backward, and the forward with 256 threads).
+int persistent_grid(int block, bool forward) {
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int warps_per_sm = 16;
+  const int warps_per_sm = forward && block <= 128 ? 20 : 16;
   return std::max(1, sms * std::max(1, warps_per_sm * 32 / block));
 }
 
@@ -178,7 +181,7 @@ int ever_trace_forward_batched(const EverBatch* batch, const float* rayo, const 
   P.max_iters = args->max_iters;
   P.out = *out;
   P.work_counter = batch->counters;
-  P.grid = persistent_grid(tn.block);
+  P.grid = persistent_grid(tn.block, true);
   const cudaError_t e = launch_forward_batched(P, deg, tn, static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? EVER_OK : set_last_error(EVER_ERR_CUDA, cudaGetErrorString(e));
 }
@@ -226,7 +229,13 @@ int ever_trace_backward_batched(const EverBatch* batch, const float* rayo, const
   P.drayo = drayo;
   P.drayd = drayd;
   P.work_counter = batch->counters + 1;
-  P.grid = persistent_grid(tn.block);
+  P.grid = persistent_grid(tn.block, false);
+  // replay order: slots grouped by their rays' event counts (longest first) over all views
+  char* scratch = static_cast<char*>(batch->order_scratch);
+  int32_t* slots = reinterpret_cast<int32_t*>(scratch + ray_order_workspace(std::max<int64_t>(batch->num_slots, 1)));
+  e = backward_slot_order(iters, batch->slot_ray, batch->num_slots, 0, scratch, slots, st);
+  if (e != cudaSuccess) return set_last_error(EVER_ERR_CUDA, cudaGetErrorString(e));
+  P.slot_order = slots;
   e = launch_backward_batched(P, deg, tn, st);
   return e == cudaSuccess ? EVER_OK : set_last_error(EVER_ERR_CUDA, cudaGetErrorString(e));
 }

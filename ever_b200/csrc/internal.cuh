@@ -45,7 +45,7 @@ cudaError_t ray_order(const float* rayo, const float* rayd, int64_t R, char* ws,
                       const uint8_t* bins = nullptr);
 // Backward launch order over forward slots: slots whose rays consumed more events first
 // (key min(iters >> shift, 255), descending), the forward's slot order inside a key.
-// Workspace: ray_order_workspace(R).
+// ray_order[s] < 0 marks a padding slot (sorted last). Workspace: ray_order_workspace(R).
 cudaError_t backward_slot_order(const int32_t* iters, const int32_t* ray_order, int64_t R, int shift, char* ws,
                                 int32_t* slot_order, cudaStream_t st);
 cudaError_t scene_build(const float* mean, const float* scale, const float* quat, const float* density,
@@ -70,6 +70,9 @@ struct FwdParams {
 };
 
 cudaError_t launch_forward(const FwdParams& P, int deg, const EverTune& tune, cudaStream_t st);
+// Per k-buffer size launchers (trace_fwd_k8.cu, trace_fwd_k16.cu, trace_fwd_k32.cu).
+template <int KBUF>
+cudaError_t launch_forward_k(const FwdParams& P, int deg, int block, int traversal, cudaStream_t st);
 
 // ---- batched persistent launches: many views over several scenes in one launch ----
 struct BatchScene {  // one row of the device-side scene table
@@ -110,12 +113,15 @@ struct BatchFwdParams {
 };
 
 cudaError_t launch_forward_batched(const BatchFwdParams& P, int deg, const EverTune& tune, cudaStream_t st);
+template <int KBUF>
+cudaError_t launch_forward_batched_k(const BatchFwdParams& P, int deg, int block, cudaStream_t st);
 
 struct BatchBwdParams {
   const BatchScene* scenes;
   const BatchView* views;
   int num_views;
   const int32_t* slot_ray;
+  const int32_t* slot_order;  // nullable: packet lane position -> slot (slots of any view)
   int64_t num_slots;
   const float* rayo;
   const float* rayd;

@@ -103,7 +103,7 @@ __global__ void k_bwd_keys(const int32_t* __restrict__ iters, const int32_t* __r
   const int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (s >= R) return;
   const int64_t r = ray_order ? int64_t(ray_order[s]) : s;
-  const uint32_t n = uint32_t(max(iters[r], 0)) >> shift;
+  const uint32_t n = r >= 0 ? uint32_t(max(iters[r], 0)) >> shift : 0u;  // padding slot: last
   keys[s] = 255u - min(n, 255u);
   vals[s] = uint32_t(s);
 }

@@ -497,7 +497,10 @@ __global__ void __launch_bounds__(256) k_trace_bwd(const BwdParams P) {
   backward_ray<DEG>(S, C, r, slot, smem + tid, blockDim.x);
 }
 
-// Persistent batched backward: warps take 32-slot packets from a device counter.
+// Persistent batched backward: warps take 32-slot packets from a device counter. With a
+// slot order the lanes of a packet may replay slots of different views and scenes (the
+// backward does not traverse, so nothing needs to be warp-uniform): each lane finds its
+// own view by binary search over the views' slot ranges.
 template <int DEG>
 __global__ void __launch_bounds__(256) k_trace_bwd_batched(const BatchBwdParams P) {
   extern __shared__ int smem[];
@@ -510,9 +513,15 @@ __global__ void __launch_bounds__(256) k_trace_bwd_batched(const BatchBwdParams 
     if (lane == 0) pk = atomicAdd(P.work_counter, 1u);
     pk = __shfl_sync(0xffffffffu, pk, 0);
     if (int64_t(pk) >= num_packets) break;
-    const int64_t slot = int64_t(pk) * 32 + lane;
-    int v = 0;
-    while (v + 1 < P.num_views && P.views[v + 1].slot_offset <= int64_t(pk) * 32) ++v;
+    const int64_t pos = int64_t(pk) * 32 + lane;
+    const int64_t slot = P.slot_order ? int64_t(P.slot_order[pos]) : pos;
+    int lo = 0, hi = P.num_views - 1;  // last view with slot_offset <= slot
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (P.views[mid].slot_offset <= slot) lo = mid;
+      else hi = mid - 1;
+    }
+    const int v = lo;
     const BatchScene bs_ = P.scenes[P.views[v].scene];
     const BScene S{reinterpret_cast<const Node*>(bs_.nodes), reinterpret_cast<const Record*>(bs_.records),
                    bs_.features, bs_.K, bs_.acc_geo, bs_.acc_feat};

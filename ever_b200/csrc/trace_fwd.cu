@@ -1,571 +1,17 @@
-// Forward trace: LBVH traversal that gathers each ray's next KBUF entry/exit events into
-// a sorted register buffer, then integrates them in order (update() with SH colour
-// evaluated along the ray), round after round.
-//
-// Two traversals share the same gather/consume semantics:
-//  - packet (default): the 32 rays of a warp walk ONE node sequence together. Each
-//    lane tests its own ray against the node's two child boxes, __ballot_sync decides
-//    where the warp goes, and a per-warp stack lives in shared memory. Node fetches
-//    are warp-uniform (one broadcast load) and the control flow never diverges.
-//  - per-ray: each thread walks the tree alone (stack in shared memory per thread).
-//
-// Reference: raygen loop splinetracers/fast_ellipsoid_splinetracer/slang/shaders.slang:171-235,
-// intersection program :84-107 and any-hit k-buffer :117-164. Our rounds gather
-// events strictly after the last gathered one in the total order (t, Morton position,
-// entry-before-exit), so no round boundary of ours drops an event; the reference's own
-// 16-event round boundaries are replayed while consuming (s16 below): an event tied with
-// the 16th event of a reference round is dropped, and an exit beyond tmax counts only
-// inside the reference round that consumed its entry. The result is the reference's
-// event sequence for any KBUF.
+// Forward trace dispatch: k-buffer size -> the instantiations in trace_fwd_k{8,16,32}.cu
+// (kernels in trace_fwd.cuh).
 #include "common.cuh"
 #include "internal.cuh"
 
 namespace ever {
-namespace {
-
-constexpr unsigned kFull = 0xffffffffu;
-constexpr int kMaxMembers = 16;
-
-template <int KBUF>
-__device__ __forceinline__ void buf_insert(uint64_t (&buf)[KBUF], uint64_t k) {
-#pragma unroll
-  for (int i = 0; i < KBUF; ++i) {
-    const uint64_t b = buf[i];
-    const bool lt = k < b;
-    buf[i] = lt ? k : b;
-    k = lt ? b : k;
-  }
-}
-
-__device__ __forceinline__ Node load_node(const Node* __restrict__ nodes, int n) {
-  const float4* p = reinterpret_cast<const float4*>(nodes + n);
-  Node nd;
-  nd.a = __ldg(p + 0);
-  nd.b = __ldg(p + 1);
-  nd.c = __ldg(p + 2);
-  nd.d = __ldg(reinterpret_cast<const int4*>(p + 3));
-  return nd;
-}
-
-struct RaySlab {
-  float3 invd, ood;
-};
-
-__device__ __forceinline__ RaySlab make_slab(const Ray& r) {
-  auto inv = [](float d) { return 1.f / (fabsf(d) > 1e-20f ? d : copysignf(1e-20f, d)); };
-  RaySlab s;
-  s.invd = make_float3(inv(r.d.x), inv(r.d.y), inv(r.d.z));
-  s.ood = make_float3(r.o.x * s.invd.x, r.o.y * s.invd.y, r.o.z * s.invd.z);
-  return s;
-}
-
-// Slab test of [lo, hi] against [tlo, thi]; returns the entry distance or +inf on a miss.
-__device__ __forceinline__ float slab(const RaySlab& s, float lx, float ly, float lz, float hx, float hy, float hz,
-                                      float tlo, float thi) {
-  const float ax = fmaf(lx, s.invd.x, -s.ood.x), bx = fmaf(hx, s.invd.x, -s.ood.x);
-  const float ay = fmaf(ly, s.invd.y, -s.ood.y), by = fmaf(hy, s.invd.y, -s.ood.y);
-  const float az = fmaf(lz, s.invd.z, -s.ood.z), bz = fmaf(hz, s.invd.z, -s.ood.z);
-  const float tn = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), tlo));
-  const float tf = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fminf(fmaxf(az, bz), thi));
-  return tn <= tf ? tn : INFINITY;
-}
-
-__device__ __forceinline__ bool box_contains(float lx, float ly, float lz, float hx, float hy, float hz, float3 p) {
-  return p.x >= lx && p.x <= hx && p.y >= ly && p.y <= hy && p.z >= lz && p.z <= hz;
-}
-
-// One leaf: the ellipsoid's entry/exit events that are candidates of this round
-// (see the file comment) go into the sorted buffer.
-template <int KBUF>
-__device__ __forceinline__ void leaf_insert(const Record* __restrict__ recs, int j, const Ray& ray, uint64_t lower,
-                                            float s16, float tmax, uint64_t (&buf)[KBUF]) {
-  const Record R = load_record(recs, j);
-  HitT H;
-  if (!intersect(R, ray, H)) return;
-  if (H.t0 > s16 && H.t0 <= tmax) {
-    const uint64_t e = event_key(H.t0, j, 0);
-    if (e > lower && e < buf[KBUF - 1]) buf_insert(buf, e);
-  }
-  if (H.t1 > s16 && (H.t1 <= tmax || (H.t0 > s16 && H.t0 <= tmax))) {
-    const uint64_t e = event_key(H.t1, j, 1);
-    if (e > lower && e < buf[KBUF - 1]) buf_insert(buf, e);
-  }
-}
-
-// ---- per-ray traversal ----
-template <int KBUF>
-__device__ void gather_ray(const Node* __restrict__ nodes, const Record* __restrict__ recs, const Ray& ray,
-                           const RaySlab& sl, uint64_t lower, float s16, float tmax, uint64_t (&buf)[KBUF],
-                           int* st_node, float* st_t, int stride, uint32_t& status) {
-  const float lo_t = fmaxf(lower ? key_t(lower) : 0.f, s16);
-  const float cap = fminf(tmax, kSentinel);
-  int sp = 0;
-  int node = 0;
-  for (;;) {
-    const Node nd = load_node(nodes, node);
-    const float hi = fminf(cap, key_t(buf[KBUF - 1]));  // an empty slot is NaN: fminf keeps cap
-    const float tc[2] = {slab(sl, nd.a.x, nd.a.y, nd.a.z, nd.a.w, nd.b.x, nd.b.y, lo_t, hi),
-                         slab(sl, nd.b.z, nd.b.w, nd.c.x, nd.c.y, nd.c.z, nd.c.w, lo_t, hi)};
-    const int c[2] = {nd.d.x, nd.d.y};
-#pragma unroll
-    for (int k = 0; k < 2; ++k)
-      if (tc[k] != INFINITY && c[k] < 0) leaf_insert(recs, ~c[k], ray, lower, s16, tmax, buf);
-    const bool i0 = tc[0] != INFINITY && c[0] >= 0;
-    const bool i1 = tc[1] != INFINITY && c[1] >= 0;
-    if (i0 && i1) {
-      const bool first0 = tc[0] <= tc[1];
-      if (sp < kStackDepth) {
-        st_node[sp * stride] = first0 ? c[1] : c[0];
-        st_t[sp * stride] = first0 ? tc[1] : tc[0];
-        ++sp;
-      } else {
-        status |= EVER_STATUS_STACK_OVERFLOW;
-      }
-      node = first0 ? c[0] : c[1];
-      continue;
-    }
-    if (i0 || i1) {
-      node = i0 ? c[0] : c[1];
-      continue;
-    }
-    bool found = false;
-    while (sp > 0) {
-      --sp;
-      if (st_t[sp * stride] <= fminf(cap, key_t(buf[KBUF - 1]))) {
-        node = st_node[sp * stride];
-        found = true;
-        break;
-      }
-    }
-    if (!found) break;
-  }
-}
-
-// ---- packet traversal: the warp walks one node sequence ----
-template <int KBUF>
-__device__ void gather_packet(const Node* __restrict__ nodes, const Record* __restrict__ recs, const Ray& ray,
-                              const RaySlab& sl, bool act, uint64_t lower, float s16, float tmax,
-                              uint64_t (&buf)[KBUF], int* wstack, int lane, uint32_t& status) {
-  const float lo_t = fmaxf(lower ? key_t(lower) : 0.f, s16);
-  const float cap = fminf(tmax, kSentinel);
-  int sp = 0;
-  int node = 0;
-  for (;;) {
-    const Node nd = load_node(nodes, node);
-    float t0 = INFINITY, t1 = INFINITY;
-    if (act) {
-      const float hi = fminf(cap, key_t(buf[KBUF - 1]));
-      t0 = slab(sl, nd.a.x, nd.a.y, nd.a.z, nd.a.w, nd.b.x, nd.b.y, lo_t, hi);
-      t1 = slab(sl, nd.b.z, nd.b.w, nd.c.x, nd.c.y, nd.c.z, nd.c.w, lo_t, hi);
-    }
-    const unsigned m0 = __ballot_sync(kFull, t0 != INFINITY);
-    const unsigned m1 = __ballot_sync(kFull, t1 != INFINITY);
-    const int c0 = nd.d.x, c1 = nd.d.y;
-    if (c0 < 0 && t0 != INFINITY) leaf_insert(recs, ~c0, ray, lower, s16, tmax, buf);
-    if (c1 < 0 && t1 != INFINITY) leaf_insert(recs, ~c1, ray, lower, s16, tmax, buf);
-    const bool g0 = c0 >= 0 && m0 != 0u, g1 = c1 >= 0 && m1 != 0u;
-    if (g0 && g1) {
-      // nearer child first, by majority of the lanes that hit either
-      const unsigned pref0 = __ballot_sync(kFull, t0 <= t1 && t0 != INFINITY);
-      const bool first0 = 2 * __popc(pref0) >= __popc(m0 | m1);
-      if (sp < kStackDepth) {
-        if (lane == 0) {
-          const int far = first0 ? c1 : c0;
-          wstack[sp] = far;
-          asm volatile("prefetch.global.L1 [%0];" ::"l"(nodes + far));
-        }
-        ++sp;
-      } else {
-        status |= EVER_STATUS_STACK_OVERFLOW;
-      }
-      __syncwarp();
-      node = first0 ? c0 : c1;
-    } else if (g0 || g1) {
-      node = g0 ? c0 : c1;
-    } else {
-      if (sp == 0) break;
-      --sp;
-      node = wstack[sp];
-    }
-  }
-}
-
-__device__ __forceinline__ void member_insert(int p, int j, int& n_mem, int (&mem_p)[kMaxMembers],
-                                              int (&mem_j)[kMaxMembers]) {
-  int jj = j;
-  for (int q = 0; q < n_mem; ++q) {
-    if (p < mem_p[q]) {
-      const int tp = mem_p[q], tj = mem_j[q];
-      mem_p[q] = p;
-      mem_j[q] = jj;
-      p = tp;
-      jj = tj;
-    }
-  }
-  mem_p[n_mem] = p;
-  mem_j[n_mem] = jj;
-  ++n_mem;
-}
-
-// Ellipsoid j contains the ray start (t0 <= 0 < t1): record it (sorted by original index);
-// beyond kMaxMembers the rest are summed into `extra` in traversal order (status flag).
-template <int DEG>
-__device__ __forceinline__ void point_leaf(const Record* __restrict__ recs, const float* __restrict__ feats, int fst,
-                                           const float* B, int bs, const Ray& ray, int j, int& n_mem,
-                                           int (&mem_p)[kMaxMembers], int (&mem_j)[kMaxMembers], float4& extra,
-                                           uint32_t& status) {
-  const Record R = load_record(recs, j);
-  HitT H;
-  if (!(intersect(R, ray, H) && H.t0 <= 0.f && H.t1 > 0.f)) return;
-  if (n_mem < kMaxMembers) {
-    member_insert(__float_as_int(R.r3.y), j, n_mem, mem_p, mem_j);
-  } else {
-    status |= EVER_STATUS_INIT_OVERFLOW;
-    const float sg = R.r3.x;
-    const float3 c = sh_colour<DEG>(feats + int64_t(j) * fst, B, bs);
-    extra.x = extra.x + sg;
-    extra.y = extra.y + sg * c.x;
-    extra.z = extra.z + sg * c.y;
-    extra.w = extra.w + sg * c.z;
-  }
-}
-
-// Point query for the ray start; PACKET: warp-uniform walk.
-template <int DEG, bool PACKET>
-__device__ int point_members(const Node* __restrict__ nodes, const Record* __restrict__ recs,
-                             const float* __restrict__ feats, int fst, const float* B, int bs, const Ray& ray, bool act,
-                             int* stack, int stride, int lane, int (&mem_p)[kMaxMembers], int (&mem_j)[kMaxMembers],
-                             float4& extra, uint32_t& status) {
-  int n_mem = 0;
-  int sp = 0;
-  int node = 0;
-  for (;;) {
-    const Node nd = load_node(nodes, node);
-    const bool h0 = act && box_contains(nd.a.x, nd.a.y, nd.a.z, nd.a.w, nd.b.x, nd.b.y, ray.o);
-    const bool h1 = act && box_contains(nd.b.z, nd.b.w, nd.c.x, nd.c.y, nd.c.z, nd.c.w, ray.o);
-    const int c0 = nd.d.x, c1 = nd.d.y;
-    if (h0 && c0 < 0) point_leaf<DEG>(recs, feats, fst, B, bs, ray, ~c0, n_mem, mem_p, mem_j, extra, status);
-    if (h1 && c1 < 0) point_leaf<DEG>(recs, feats, fst, B, bs, ray, ~c1, n_mem, mem_p, mem_j, extra, status);
-    bool g0 = h0 && c0 >= 0, g1 = h1 && c1 >= 0;
-    if (PACKET) {
-      g0 = __any_sync(kFull, g0);
-      g1 = __any_sync(kFull, g1);
-    }
-    if (g0 && g1) {
-      if (sp < kStackDepth) {
-        if (!PACKET || lane == 0) stack[sp * stride] = c1;
-        ++sp;
-      } else {
-        status |= EVER_STATUS_STACK_OVERFLOW;
-      }
-      if (PACKET) __syncwarp();
-      node = c0;
-    } else if (g0 || g1) {
-      node = g0 ? c0 : c1;
-    } else {
-      if (sp == 0) break;
-      --sp;
-      node = stack[sp * stride];
-    }
-  }
-  return n_mem;
-}
-
-// Which scene a packet traces, and the per-launch constants.
-struct SceneRef {
-  const Node* nodes;
-  const Record* recs;
-  const float* features;
-  int64_t N;
-  int K;
-};
-
-struct TraceCtx {
-  float tmin, tmax;
-  int max_iters;
-  int64_t log_stride;  // event-log row length (slots)
-  EverForwardOut out;
-};
-
-// Integrates the gathered events in order. Returns true once the ray is finished.
-template <int KBUF, int DEG>
-__device__ __forceinline__ bool consume(const SceneRef& sc, const TraceCtx& C, const Ray& ray, const float* B,
-                                        int bs, int64_t slot, uint64_t (&buf)[KBUF], State& s, float4& last_dirac,
-                                        int& iters, float& s16, int& cnt16, uint64_t& lower, uint32_t& status) {
-  const int fst = feat_stride(sc.K);
-  const uint64_t last = buf[KBUF - 1];
-  bool done = false;
-  for (int n = 0; n < KBUF && !done; ++n) {
-    const uint64_t k = buf[0];
-#pragma unroll
-    for (int i = 0; i < KBUF - 1; ++i) buf[i] = buf[i + 1];
-    buf[KBUF - 1] = kEmptyKey;
-    if (k == kEmptyKey) return true;  // nothing left beyond the last gathered event
-    const float t = key_t(k);
-    const int j = key_pos(k);
-    const int ex = key_exit(k);
-    if (!(t > s16)) continue;  // tied with the 16th event of a reference round: dropped
-    if (t > kSentinel) return true;
-    const float4 r3 = __ldg(&sc.recs[j].r3);
-    if (ex && t > C.tmax) {
-      HitT H;
-      intersect(load_record(sc.recs, j), ray, H);
-      if (!(H.t0 > s16 && H.t0 <= C.tmax)) continue;
-    }
-    const float3 c = sh_colour<DEG>(sc.features + int64_t(j) * fst, B, bs);
-    const float dh = ex ? -r3.x : r3.x;
-    const float4 dirac = make_float4(dh, dh * c.x, dh * c.y, dh * c.z);
-    update(s, t, dirac);
-    last_dirac = dirac;
-    if (C.out.event_log) {
-      if (iters < C.out.log_cap)
-        C.out.event_log[int64_t(iters) * C.log_stride + slot] = 2 * j + (ex ? 0 : 1);
-      else
-        status |= EVER_STATUS_LOG_OVERFLOW;
-    }
-    if (C.out.touch_count) atomicAdd(C.out.touch_count + __float_as_int(r3.y), 1);
-    ++iters;
-    if (++cnt16 == kRefRound) {
-      s16 = t;
-      cnt16 = 0;
-    }
-    if (!(s.logT < kLogCutoff && iters < C.max_iters)) done = true;
-  }
-  if (done || last == kEmptyKey) return true;
-  lower = last;
-  return false;
-}
-
-template <int DEG>
-__device__ __forceinline__ void init_density(const SceneRef& sc, const float* B, int bs, int n_mem,
-                                             const int (&mem_j)[kMaxMembers], float4 extra, uint32_t status,
-                                             State& s) {
-  const int fst = feat_stride(sc.K);
-  for (int q = 0; q < n_mem; ++q) {
-    const int j = mem_j[q];
-    const float sg = __ldg(&sc.recs[j].r3.x);
-    const float3 c = sh_colour<DEG>(sc.features + int64_t(j) * fst, B, bs);
-    s.drgb.x = s.drgb.x + sg;
-    s.drgb.y = s.drgb.y + sg * c.x;
-    s.drgb.z = s.drgb.z + sg * c.y;
-    s.drgb.w = s.drgb.w + sg * c.z;
-  }
-  if (status & EVER_STATUS_INIT_OVERFLOW) {
-    s.drgb.x = s.drgb.x + extra.x;
-    s.drgb.y = s.drgb.y + extra.y;
-    s.drgb.z = s.drgb.z + extra.z;
-    s.drgb.w = s.drgb.w + extra.w;
-  }
-}
-
-__device__ __forceinline__ void write_outputs(const EverForwardOut& out, int64_t r, const State& s, float4 last_dirac,
-                                              int iters, uint32_t status) {
-  float* o = out.out + 5 * r;
-  o[0] = s.C.x;
-  o[1] = s.C.y;
-  o[2] = s.C.z;
-  o[3] = 1.f - expf(-s.logT);
-  o[4] = s.dist_x - s.dist_y;
-  if (out.states) {
-    float4* st = reinterpret_cast<float4*>(out.states + 16 * r);
-    st[0] = make_float4(s.dist_x, s.dist_y, s.cum_x, s.cum_y);
-    st[1] = make_float4(0.f, 0.f, 0.f, s.t);
-    st[2] = s.drgb;
-    st[3] = make_float4(s.logT, s.C.x, s.C.y, s.C.z);
-  }
-  if (out.last_dirac) reinterpret_cast<float4*>(out.last_dirac)[r] = last_dirac;
-  out.iters[r] = iters;
-  if (out.ray_stats) {
-    out.ray_stats[2 * r] = float(iters);
-    out.ray_stats[2 * r + 1] = s.t;
-  }
-  if (status && out.status) atomicOr(out.status, int(status));
-}
-
-__device__ __forceinline__ Ray load_ray(const float* rayo, const float* rayd, int64_t r, float tmin) {
-  const float3 ro = make_float3(rayo[3 * r], rayo[3 * r + 1], rayo[3 * r + 2]);
-  const float3 rd = make_float3(rayd[3 * r], rayd[3 * r + 1], rayd[3 * r + 2]);
-  return make_ray(ro, rd, tmin);
-}
-
-__device__ __forceinline__ SceneRef scene_of(const FwdParams& P) {
-  return SceneRef{reinterpret_cast<const Node*>(P.nodes), reinterpret_cast<const Record*>(P.records), P.features,
-                  P.N, P.K};
-}
-
-template <int KBUF, int DEG>
-__global__ void __launch_bounds__(256) k_trace_fwd_ray(const FwdParams P) {
-  extern __shared__ int smem[];
-  const int tid = threadIdx.x, stride = blockDim.x;
-  int* st_node = smem + tid;
-  float* st_t = reinterpret_cast<float*>(smem + kStackDepth * stride) + tid;
-  const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;
-  if (gi >= P.R) return;
-  const int64_t r = P.ray_order ? int64_t(P.ray_order[gi]) : gi;
-  const SceneRef sc = scene_of(P);
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out};
-  const Ray ray = load_ray(P.rayo, P.rayd, r, P.tmin);
-  const RaySlab sl = make_slab(ray);
-  float B[16];
-  sh_basis<DEG>(ray.rd, B);
-  uint32_t status = 0;
-  State s = empty_state();
-  float4 last_dirac = make_float4(0.f, 0.f, 0.f, 0.f);
-  int iters = 0;
-  if (sc.N > 0) {
-    int mem_p[kMaxMembers], mem_j[kMaxMembers];
-    float4 extra = make_float4(0.f, 0.f, 0.f, 0.f);
-    const int n_mem = point_members<DEG, false>(sc.nodes, sc.recs, sc.features, feat_stride(sc.K), B, 1, ray, true,
-                                                st_node, stride, 0, mem_p, mem_j, extra, status);
-    init_density<DEG>(sc, B, 1, n_mem, mem_j, extra, status, s);
-    float s16 = 0.f;
-    int cnt16 = 0;
-    uint64_t lower = 0;
-    bool done = C.max_iters <= 0;
-    while (!done) {
-      uint64_t buf[KBUF];
-#pragma unroll
-      for (int i = 0; i < KBUF; ++i) buf[i] = kEmptyKey;
-      gather_ray<KBUF>(sc.nodes, sc.recs, ray, sl, lower, s16, C.tmax, buf, st_node, st_t, stride, status);
-      done = consume<KBUF, DEG>(sc, C, ray, B, 1, gi, buf, s, last_dirac, iters, s16, cnt16, lower, status);
-    }
-  }
-  write_outputs(C.out, r, s, last_dirac, iters, status);
-}
-
-// One warp traces one packet of up to 32 rays against one scene (lanes with valid=false
-// only take part in the warp-wide votes).
-template <int KBUF, int DEG>
-__device__ __forceinline__ void trace_packet(const SceneRef& sc, const TraceCtx& C, const float* rayo,
-                                             const float* rayd, int64_t r, bool valid, int64_t slot, int* wstack,
-                                             float* B, int bs, int lane) {
-  const Ray ray = load_ray(rayo, rayd, valid ? r : 0, C.tmin);
-  const RaySlab sl = make_slab(ray);
-  {
-    float Bl[16];
-    sh_basis<DEG>(ray.rd, Bl);
-#pragma unroll
-    for (int k = 0; k < (DEG + 1) * (DEG + 1); ++k) B[k * bs] = Bl[k];
-  }
-  uint32_t status = 0;
-  State s = empty_state();
-  float4 last_dirac = make_float4(0.f, 0.f, 0.f, 0.f);
-  int iters = 0;
-  if (sc.N > 0) {
-    int mem_p[kMaxMembers], mem_j[kMaxMembers];
-    float4 extra = make_float4(0.f, 0.f, 0.f, 0.f);
-    const int n_mem = point_members<DEG, true>(sc.nodes, sc.recs, sc.features, feat_stride(sc.K), B, bs, ray, valid,
-                                               wstack, 1, lane, mem_p, mem_j, extra, status);
-    init_density<DEG>(sc, B, bs, n_mem, mem_j, extra, status, s);
-    float s16 = 0.f;
-    int cnt16 = 0;
-    uint64_t lower = 0;
-    bool act = valid && C.max_iters > 0;
-    while (__any_sync(kFull, act)) {
-      uint64_t buf[KBUF];
-#pragma unroll
-      for (int i = 0; i < KBUF; ++i) buf[i] = kEmptyKey;
-      gather_packet<KBUF>(sc.nodes, sc.recs, ray, sl, act, lower, s16, C.tmax, buf, wstack, lane, status);
-      if (act) act = !consume<KBUF, DEG>(sc, C, ray, B, bs, slot, buf, s, last_dirac, iters, s16, cnt16, lower, status);
-    }
-  }
-  if (valid) write_outputs(C.out, r, s, last_dirac, iters, status);
-  __syncwarp();
-}
-
-template <int KBUF, int DEG>
-__global__ void __launch_bounds__(256) k_trace_fwd_packet(const FwdParams P) {
-  extern __shared__ int smem[];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  int* wstack = smem + warp * kStackDepth;
-  float* B = reinterpret_cast<float*>(smem + (blockDim.x / 32) * kStackDepth) + tid;  // B[k * blockDim.x]
-  const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;
-  const bool valid = gi < P.R;  // every lane stays for the warp-wide ballots
-  const int64_t r = valid ? (P.ray_order ? int64_t(P.ray_order[gi]) : gi) : 0;
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out};
-  trace_packet<KBUF, DEG>(scene_of(P), C, P.rayo, P.rayd, r, valid, gi, wstack, B, blockDim.x, lane);
-}
-
-// Persistent batched forward: warps take 32-slot packets from a device counter until
-// all views are done. Each packet lies inside one view, hence one scene.
-template <int KBUF, int DEG>
-__global__ void __launch_bounds__(256) k_trace_fwd_batched(const BatchFwdParams P) {
-  extern __shared__ int smem[];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  int* wstack = smem + warp * kStackDepth;
-  float* B = reinterpret_cast<float*>(smem + (blockDim.x / 32) * kStackDepth) + tid;
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.num_slots, P.out};
-  const int64_t num_packets = P.num_slots / 32;
-  for (;;) {
-    unsigned int pk = 0;
-    if (lane == 0) pk = atomicAdd(P.work_counter, 1u);
-    pk = __shfl_sync(kFull, pk, 0);
-    if (int64_t(pk) >= num_packets) break;
-    const int64_t slot = int64_t(pk) * 32 + lane;
-    int v = 0;  // the view holding this packet (few views: linear scan, warp-uniform)
-    while (v + 1 < P.num_views && P.views[v + 1].slot_offset <= int64_t(pk) * 32) ++v;
-    const BatchScene bs_ = P.scenes[P.views[v].scene];
-    const SceneRef sc{reinterpret_cast<const Node*>(bs_.nodes), reinterpret_cast<const Record*>(bs_.records),
-                      bs_.features, bs_.N, bs_.K};
-    const int32_t r = P.slot_ray[slot];
-    trace_packet<KBUF, DEG>(sc, C, P.rayo, P.rayd, r, r >= 0, slot, wstack, B, blockDim.x, lane);
-  }
-}
-
-template <int KBUF, int DEG>
-cudaError_t launch_t(const FwdParams& P, int block, int traversal, cudaStream_t st) {
-  const int64_t grid = (P.R + block - 1) / block;
-  if (traversal == 1) {
-    const size_t smem = size_t(kStackDepth) * block * (sizeof(int) + sizeof(float));
-    auto kern = k_trace_fwd_ray<KBUF, DEG>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return e;
-    kern<<<unsigned(grid), block, smem, st>>>(P);
-  } else {
-    const size_t smem = size_t(kStackDepth) * (block / 32) * sizeof(int) + size_t(16) * block * sizeof(float);
-    k_trace_fwd_packet<KBUF, DEG><<<unsigned(grid), block, smem, st>>>(P);
-  }
-  return cudaGetLastError();
-}
-
-template <int KBUF>
-cudaError_t launch_k(const FwdParams& P, int deg, int block, int traversal, cudaStream_t st) {
-  switch (deg) {
-    case 0: return launch_t<KBUF, 0>(P, block, traversal, st);
-    case 1: return launch_t<KBUF, 1>(P, block, traversal, st);
-    case 2: return launch_t<KBUF, 2>(P, block, traversal, st);
-    default: return launch_t<KBUF, 3>(P, block, traversal, st);
-  }
-}
-
-template <int KBUF, int DEG>
-cudaError_t launch_batched_t(const BatchFwdParams& P, int block, cudaStream_t st) {
-  const size_t smem = size_t(kStackDepth) * (block / 32) * sizeof(int) + size_t(16) * block * sizeof(float);
-  cudaError_t e = cudaMemsetAsync(P.work_counter, 0, sizeof(unsigned int), st);
-  if (e != cudaSuccess) return e;
-  k_trace_fwd_batched<KBUF, DEG><<<P.grid, block, smem, st>>>(P);
-  return cudaGetLastError();
-}
-
-template <int KBUF>
-cudaError_t launch_batched_k(const BatchFwdParams& P, int deg, int block, cudaStream_t st) {
-  switch (deg) {
-    case 0: return launch_batched_t<KBUF, 0>(P, block, st);
-    case 1: return launch_batched_t<KBUF, 1>(P, block, st);
-    case 2: return launch_batched_t<KBUF, 2>(P, block, st);
-    default: return launch_batched_t<KBUF, 3>(P, block, st);
-  }
-}
-
-}  // namespace
 
 cudaError_t launch_forward_batched(const BatchFwdParams& P, int deg, const EverTune& tune, cudaStream_t st) {
   if (P.num_slots == 0) return cudaSuccess;
   const int block = tune.block > 0 ? tune.block : 128;
   switch (tune.kbuf) {
-    case 8: return launch_batched_k<8>(P, deg, block, st);
-    case 32: return launch_batched_k<32>(P, deg, block, st);
-    default: return launch_batched_k<16>(P, deg, block, st);
+    case 8: return launch_forward_batched_k<8>(P, deg, block, st);
+    case 32: return launch_forward_batched_k<32>(P, deg, block, st);
+    default: return launch_forward_batched_k<16>(P, deg, block, st);
   }
 }
 
@@ -573,9 +19,9 @@ cudaError_t launch_forward(const FwdParams& P, int deg, const EverTune& tune, cu
   if (P.R == 0) return cudaSuccess;
   const int block = tune.block > 0 ? tune.block : 128;
   switch (tune.kbuf) {
-    case 8: return launch_k<8>(P, deg, block, tune.traversal, st);
-    case 32: return launch_k<32>(P, deg, block, tune.traversal, st);
-    default: return launch_k<16>(P, deg, block, tune.traversal, st);
+    case 8: return launch_forward_k<8>(P, deg, block, tune.traversal, st);
+    case 32: return launch_forward_k<32>(P, deg, block, tune.traversal, st);
+    default: return launch_forward_k<16>(P, deg, block, tune.traversal, st);
   }
 }
 

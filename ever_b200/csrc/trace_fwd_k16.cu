@@ -1,0 +1,16 @@
+// Forward trace kernels with a 16-event buffer (trace_fwd.cuh).
+#include "trace_fwd.cuh"
+
+namespace ever {
+
+template <>
+cudaError_t launch_forward_k<16>(const FwdParams& P, int deg, int block, int traversal, cudaStream_t st) {
+  return launch_k<16>(P, deg, block, traversal, st);
+}
+
+template <>
+cudaError_t launch_forward_batched_k<16>(const BatchFwdParams& P, int deg, int block, cudaStream_t st) {
+  return launch_batched_k<16>(P, deg, block, st);
+}
+
+}  // namespace ever

@@ -1,0 +1,16 @@
+// Forward trace kernels with a 8-event buffer (trace_fwd.cuh).
+#include "trace_fwd.cuh"
+
+namespace ever {
+
+template <>
+cudaError_t launch_forward_k<8>(const FwdParams& P, int deg, int block, int traversal, cudaStream_t st) {
+  return launch_k<8>(P, deg, block, traversal, st);
+}
+
+template <>
+cudaError_t launch_forward_batched_k<8>(const BatchFwdParams& P, int deg, int block, cudaStream_t st) {
+  return launch_batched_k<8>(P, deg, block, st);
+}
+
+}  // namespace ever
