@@ -52,6 +52,11 @@ class EverMlp(ctypes.Structure):
     _fields_ = [("params", c_p), ("w1", c_p), ("w2", c_p), ("w3", c_p), ("centre", c_f32 * 3), ("inv_scale", c_f32)]
 
 
+class EverCamera(ctypes.Structure):
+    _fields_ = [("width", c_i32), ("height", c_i32), ("fx", c_f32), ("fy", c_f32), ("cx", c_f32), ("cy", c_f32),
+                ("c2w", c_f32 * 12)]
+
+
 MLP_PARAMS = 9360
 
 STATUS_STACK_OVERFLOW = 1
@@ -65,6 +70,7 @@ SIGNATURES = {
     "ever_scene_workspace_bytes": (c_sz, [c_i64, c_i32]),
     "ever_scene_build": (ctypes.c_int, [c_p, c_p, c_p, c_p, c_p, c_i64, c_i32, c_p, c_sz,
                                         ctypes.POINTER(EverScene), c_p]),
+    "ever_scene_refit": (ctypes.c_int, [c_p, c_p, c_p, c_p, c_p, c_p, c_sz, ctypes.POINTER(EverScene), c_p]),
     "ever_scene_set_features": (ctypes.c_int, [ctypes.POINTER(EverScene), c_p, c_p]),
     "ever_trace_forward": (ctypes.c_int, [ctypes.POINTER(EverScene), c_p, c_p, c_i64, ctypes.POINTER(EverTraceArgs),
                                           c_p, ctypes.POINTER(EverTune), ctypes.POINTER(EverForwardOut), c_p]),
@@ -102,6 +108,11 @@ SIGNATURES = {
                                           c_p, c_p, c_p, c_sz, c_p, c_p]),
     "ever_mlp_adam": (ctypes.c_int, [ctypes.POINTER(EverMlp), c_p, c_p, c_p, c_f32, c_f32, c_f32, c_f32, c_i32,
                                      c_p]),
+    "ever_ply_count": (c_i64, [ctypes.c_char_p]),
+    "ever_ply_read": (ctypes.c_int, [ctypes.c_char_p, c_i64, c_p, c_p, c_p, c_p, c_p]),
+    "ever_sh_prepass": (ctypes.c_int, [c_p, c_p, c_i64, c_i32, c_i32, c_p, c_i32, c_p, c_p]),
+    "ever_sh_prepass_backward": (ctypes.c_int, [c_p, c_p, c_i64, c_i32, c_i32, c_p, c_i32, c_p, c_p, c_p]),
+    "ever_camera_rays": (ctypes.c_int, [ctypes.POINTER(EverCamera), c_p, c_p, c_p, c_p]),
     "ever_ray_order_binned": (ctypes.c_int, [c_p, c_p, c_p, c_i64, c_p, c_sz, c_p, c_p]),
     "ever_batch_order_binned": (ctypes.c_int, [ctypes.POINTER(EverBatch), c_p, c_p, c_p, c_p]),
 }

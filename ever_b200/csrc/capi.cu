@@ -89,6 +89,22 @@ int ever_scene_set_features(EverScene* scene, const float* features, void* strea
                      "ever_scene_set_features");
 }
 
+int ever_scene_refit(const float* mean, const float* scale, const float* quat, const float* density,
+                     const float* features, void* workspace, size_t workspace_bytes, EverScene* scene, void* stream) {
+  if (!scene) return fail(EVER_ERR_INVALID, "scene is null");
+  const int64_t N = scene->num_prims;
+  if (N == 0) return EVER_OK;
+  if (!mean || !scale || !quat || !density) return fail(EVER_ERR_INVALID, "null ellipsoid parameter pointer");
+  const ever::SceneLayout L = ever::scene_layout(N, scene->sh_coeffs);
+  char* ws = static_cast<char*>(workspace);
+  if (!ws || workspace_bytes < size_t(L.total)) return fail(EVER_ERR_WORKSPACE, "scene workspace too small");
+  if (scene->nodes != ws + L.nodes || scene->records != ws + L.records)
+    return fail(EVER_ERR_INVALID, "scene was not built on this workspace");
+  return cuda_status(ever::scene_refit(mean, scale, quat, density, features, ws, L, scene,
+                                       static_cast<cudaStream_t>(stream)),
+                     "ever_scene_refit");
+}
+
 int ever_trace_forward(const EverScene* scene, const float* rayo, const float* rayd, int64_t num_rays,
                        const EverTraceArgs* args, const int32_t* ray_order, const EverTune* tune,
                        const EverForwardOut* out, void* stream) {

@@ -52,6 +52,8 @@ cudaError_t scene_build(const float* mean, const float* scale, const float* quat
                         const float* feat, int64_t N, int K, char* ws, const SceneLayout& L, EverScene* sc,
                         cudaStream_t st);
 cudaError_t scene_set_features(EverScene* sc, const float* feat, cudaStream_t st);
+cudaError_t scene_refit(const float* mean, const float* scale, const float* quat, const float* density,
+                        const float* feat, char* ws, const SceneLayout& L, EverScene* sc, cudaStream_t st);
 
 struct FwdParams {
   const void* nodes;
@@ -226,5 +228,17 @@ cudaError_t launch_mlp_reduce(const float* partial, int grid, float* grads, floa
 cudaError_t launch_mlp_adam(float* params, const float* grads, float* m, float* v, void* w1, void* w2, void* w3,
                             float lr, float beta1, float beta2, float eps, int step, cudaStream_t st);
 cudaError_t launch_mlp_pack(const float* params, void* w1, void* w2, void* w3, cudaStream_t st);
+
+// ---- colour pre-pass and camera rays (shprep.cu) ----
+// grad_out == nullptr: forward (out = colour or features); else backward (out = grad_features).
+cudaError_t launch_sh_prepass(const float* mean, const float* feat, int64_t N, int K, int deg, const float* cam,
+                              int mode, const float* grad_out, float* out, cudaStream_t st);
+
+struct CameraParams {
+  int width, height;
+  float fx, fy, cx, cy;
+  float c2w[12];
+};
+cudaError_t launch_camera_rays(const CameraParams& C, const float* jitter, float* rayo, float* rayd, cudaStream_t st);
 
 }  // namespace ever

@@ -511,6 +511,40 @@ cudaError_t scene_build(const float* mean, const float* scale, const float* quat
   return cudaGetLastError();
 }
 
+// Refit a built scene to new ellipsoid parameters: same Morton order and tree topology as
+// the last build (the parent links stay in the workspace), new records, boxes and, when
+// given, features. Tree quality degrades as ellipsoids move far from where they were
+// built; a rebuild restores it.
+cudaError_t scene_refit(const float* mean, const float* scale, const float* quat, const float* density,
+                        const float* feat, char* ws, const SceneLayout& L, EverScene* sc, cudaStream_t st) {
+  const int64_t N = sc->num_prims;
+  const int K = sc->sh_coeffs;
+  if (N == 0) return cudaSuccess;
+  Node* nodes = reinterpret_cast<Node*>(ws + L.nodes);
+  float4* aabb_a = reinterpret_cast<float4*>(ws + L.aabb_a);
+  float4* aabb_b = reinterpret_cast<float4*>(ws + L.aabb_b);
+  uint32_t* bounds = reinterpret_cast<uint32_t*>(ws + L.bounds);
+  int32_t* pn = reinterpret_cast<int32_t*>(ws + L.parent_node);
+  int32_t* pl = reinterpret_cast<int32_t*>(ws + L.parent_leaf);
+  uint32_t* flags = reinterpret_cast<uint32_t*>(ws + L.flags);
+  const int tb = 256;
+  const int64_t gb = div_up(N, tb);
+  k_aabbs<<<unsigned(gb), tb, 0, st>>>(mean, scale, quat, N, aabb_a, bounds);
+  k_gather<<<unsigned(gb), tb, 0, st>>>(reinterpret_cast<const uint32_t*>(sc->order), N, K, mean, scale, quat, density,
+                                        aabb_a, aabb_b, reinterpret_cast<Record*>(sc->records), sc->features,
+                                        sc->order);
+  if (feat)
+    k_gather_features<<<unsigned(div_up(N * feat_stride(K), tb)), tb, 0, st>>>(sc->order, N, K, feat, sc->features);
+  if (N == 1) {
+    k_single_leaf<<<1, 1, 0, st>>>(nodes, aabb_b);
+    return cudaGetLastError();
+  }
+  cudaError_t e = cudaMemsetAsync(flags, 0, (N - 1) * sizeof(uint32_t), st);
+  if (e != cudaSuccess) return e;
+  k_refit<<<unsigned(gb), tb, 0, st>>>(N, nodes, aabb_b, pn, pl, flags);
+  return cudaGetLastError();
+}
+
 cudaError_t scene_set_features(EverScene* sc, const float* feat, cudaStream_t st) {
   const int64_t total = sc->num_prims * int64_t(sc->sh_coeffs) * 3;
   if (total == 0) return cudaSuccess;

@@ -92,6 +92,16 @@ class Scene:
                                               self.sh_coeffs, N.ptr(self.workspace), int(self.workspace.numel()),
                                               ctypes.byref(self.c), _stream(self.device)))
 
+    def refit(self, with_features=True):
+        """Refits the BVH in place to the (updated) input tensors, keeping the last build's
+        Morton order and tree topology: cheaper than rebuild() between small updates."""
+        m, s, q, d, f = self.tensors
+        with torch.cuda.device(self.device):
+            N.check(N.load().ever_scene_refit(N.ptr(m), N.ptr(s), N.ptr(q), N.ptr(d),
+                                              N.ptr(f) if with_features else None, N.ptr(self.workspace),
+                                              int(self.workspace.numel()), ctypes.byref(self.c),
+                                              _stream(self.device)))
+
     def set_features(self, features):
         _check_tensor("colors", features, self.device, 3)
         if features.shape[0] != self.num_prims or features.shape[1] != self.sh_coeffs:

@@ -115,6 +115,15 @@ int ever_scene_build(const float* mean, const float* scale, const float* quat, c
  * Counterpart of Primitives.set_features + Forward.update_model (py_binding.cpp:133-138, 207-209). */
 int ever_scene_set_features(EverScene* scene, const float* features, void* stream);
 
+/* Refits a scene built by ever_scene_build on the same workspace to new ellipsoid
+ * parameters (same N and K): records, boxes and (when features is not NULL) features are
+ * recomputed, the tree keeps the last build's Morton order and topology and is refitted
+ * bottom-up. Much cheaper than a rebuild between small parameter updates (training steps);
+ * traversal gets slower as ellipsoids move far from where they were built. No counterpart
+ * in the reference, which rebuilds its GAS on every call (GAS.cpp:56-154). */
+int ever_scene_refit(const float* mean, const float* scale, const float* quat, const float* density,
+                     const float* features, void* workspace, size_t workspace_bytes, EverScene* scene, void* stream);
+
 /* Forward trace of R rays: rayo/rayd (R,3). Counterpart of Forward.trace_rays
  * (py_binding.cpp:210-258, Forward.cpp:23-82, shaders.slang:171-235), including the
  * initial density of rays that start inside ellipsoids (initialize_density.cu:152-208).
@@ -309,6 +318,52 @@ int ever_ray_order_binned(const float* rayo, const float* rayd, const uint8_t* b
 /* ever_batch_order with cost bins: inside every view, costlier bins first. */
 int ever_batch_order_binned(const EverBatch* batch, const float* rayo, const float* rayd, const uint8_t* bins,
                             void* stream);
+
+/* ---- trained scenes from binary PLY files (host code) ----
+ * The reference's scene file layout and conversion (ply_file_loader.cc:166-293): per vertex
+ * 62 little-endian floats (mean, normal, 48 SH values, opacity, scale, rotation), turned
+ * into means, quaternions q/(q.q), scales min(softplus(s)+3e-4, 25), densities
+ * -log(1 - 0.99 sigmoid(opacity)) / (2 min scale) and SH features (N,16,3). */
+
+/* Number of ellipsoids in the file, or -1 (see ever_last_error) if it is not a valid file. */
+int64_t ever_ply_count(const char* path);
+
+/* Reads the file into HOST buffers of `capacity` ellipsoids: mean (N,3), scale (N,3),
+ * quat (N,4), density (N), features (N,16,3). */
+int ever_ply_read(const char* path, int64_t capacity, float* mean, float* scale, float* quat, float* density,
+                  float* features);
+
+/* ---- the trainer's per-ellipsoid colour pre-pass and camera ray generation ---- */
+
+/* Colour of each ellipsoid seen from the camera centre cam_pos (device, 3 floats): SH of
+ * degree sh_degree (features (N,K,3), K >= (sh_degree+1)^2) in the direction
+ * normalize(mean - cam_pos), plus 0.5. Counterpart of eval_sh.EvalSH.forward / sh_kernel
+ * (eval_sh.py:28-56, sh_kernel.slang:21-43). mode 0 writes that colour (N,3); mode 1 writes
+ * the trainer's tracer features RGB2SH(softplus(colour, beta=10)) (N,1,3) in the same pass
+ * (integration_utils/gaussian_renderer/ever.py:178-180). */
+int ever_sh_prepass(const float* mean, const float* features, int64_t num_prims, int32_t sh_coeffs,
+                    int32_t sh_degree, const float* cam_pos, int32_t mode, float* out, void* stream);
+
+/* Gradient of ever_sh_prepass with respect to the features, written in full to
+ * grad_features (N,K,3) (entries of degree > sh_degree are zero). Counterpart of
+ * EvalSH.backward / bw_sh_kernel (eval_sh.py:58-69, sh_kernel.slang:45-99), including its
+ * skip of ellipsoids whose colour gradient is below 1e-8 in every channel. */
+int ever_sh_prepass_backward(const float* mean, const float* features, int64_t num_prims, int32_t sh_coeffs,
+                             int32_t sh_degree, const float* cam_pos, int32_t mode, const float* grad_out,
+                             float* grad_features, void* stream);
+
+typedef struct EverCamera {
+  int32_t width, height;
+  float fx, fy;     /* focal lengths in pixels */
+  float cx, cy;     /* principal point in pixels (the reference uses width/2, height/2) */
+  float c2w[12];    /* camera-to-world 3x4, row-major: rayd = c2w[:, :3] d, rayo = c2w[:, 3] */
+} EverCamera;
+
+/* One ray per pixel, row-major: d = normalize(((col + ox) - cx) / fx, ((row + oy) - cy) / fy, 1),
+ * rayd = R d, rayo = camera centre. jitter (nullable, device (width*height, 2)) gives the
+ * per-pixel offsets (ox, oy); NULL means pixel centres (0.5, 0.5). Counterpart of
+ * camera2rays / get_ray_directions / get_rays (integration_utils/gaussian_renderer/ever.py:29-74,105-118). */
+int ever_camera_rays(const EverCamera* camera, const float* jitter, float* rayo, float* rayd, void* stream);
 
 #ifdef __cplusplus
 }
