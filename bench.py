@@ -196,9 +196,17 @@ def run_once(args):
     scene = T.Scene(t(sc.mean), t(sc.scale), t(sc.quat), t(sc.density.reshape(-1)), t(sc.features))
     order = T.ray_order(rayo, rayd)
     fwd = T.forward(scene, rayo, rayd, 0.0, 1000.0, 500, ray_order=order, tune=tune)
+    slots = T.backward_order(fwd, order, 0)
     T.backward(scene, rayo, rayd, fwd, torch.ones((rayo.shape[0], 5), device=dev), 0.0, 1000.0, 500,
-               ray_order=order, tune=tune)
+               ray_order=order, tune=tune, slot_order=slots)
+    # the ray-cost model on the same rays: one inference pass and one training-gradient pass
+    from ever_b200 import scheduler as SCH
+    stats = T.forward(scene, rayo, rayd, 0.0, 1000.0, 500, log_events=False, ray_stats=True, ray_order=order)
+    cm = SCH.CostModel(scale=2.0, seed=1, device=dev)
+    cm.predict(rayo, rayd, thresholds=[2.0, 2.5, 3.0])
+    cm.gradients(rayo, rayd, SCH.cost_targets(stats.ray_stats, rayo, rayd, scale=2.0))
     torch.cuda.synchronize()
+    cm.check()
     print(json.dumps({"once": True, "rays": int(rayo.shape[0]), "status": int(fwd.status.item()),
                       "events_per_ray": float(fwd.iters.float().mean().item())}))
 
