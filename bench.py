@@ -255,7 +255,9 @@ def leg_batched(dev, reps=3):
         return int(bt.status.item())
 
     best, timings = AT.autotune(run_cand, AT.workload_key(sum(int(s[0].shape[0]) for s in scenes), R, 16, dev),
-                                candidates=[c for c in AT.DEFAULT_CANDIDATES if c.ordered], warmup=1, reps=1,
+                                # the batched kernels always use warp packets: no per-ray traversal
+                                candidates=[c for c in AT.DEFAULT_CANDIDATES if c.ordered and c.traversal == 0],
+                                warmup=1, reps=1,
                                 force=True)
     tune = best.tune()
     bt = BatchedTracer(scenes, views, max_iters=500, tune=tune, graph=True)
