@@ -230,10 +230,11 @@ int ever_trace_backward_batched(const EverBatch* batch, const float* rayo, const
   P.drayd = drayd;
   P.work_counter = batch->counters + 1;
   P.grid = persistent_grid(tn.block, false);
-  // replay order: slots grouped by their rays' event counts (longest first) over all views
+  // replay order: inside each view, slots grouped by their rays' event counts (longest first)
   char* scratch = static_cast<char*>(batch->order_scratch);
   int32_t* slots = reinterpret_cast<int32_t*>(scratch + ray_order_workspace(std::max<int64_t>(batch->num_slots, 1)));
-  e = backward_slot_order(iters, batch->slot_ray, batch->num_slots, 0, scratch, slots, st);
+  e = backward_slot_order(iters, batch->slot_ray, batch->num_slots, 0, scratch, slots, st,
+                          static_cast<const BatchView*>(batch->view_table), batch->num_views);
   if (e != cudaSuccess) return set_last_error(EVER_ERR_CUDA, cudaGetErrorString(e));
   P.slot_order = slots;
   e = launch_backward_batched(P, deg, tn, st);

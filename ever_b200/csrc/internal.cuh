@@ -47,7 +47,8 @@ cudaError_t ray_order(const float* rayo, const float* rayd, int64_t R, char* ws,
 // (key min(iters >> shift, 255), descending), the forward's slot order inside a key.
 // ray_order[s] < 0 marks a padding slot (sorted last). Workspace: ray_order_workspace(R).
 cudaError_t backward_slot_order(const int32_t* iters, const int32_t* ray_order, int64_t R, int shift, char* ws,
-                                int32_t* slot_order, cudaStream_t st);
+                                int32_t* slot_order, cudaStream_t st, const BatchView* views = nullptr,
+                                int num_views = 0);
 cudaError_t scene_build(const float* mean, const float* scale, const float* quat, const float* density,
                         const float* feat, int64_t N, int K, char* ws, const SceneLayout& L, EverScene* sc,
                         cudaStream_t st);

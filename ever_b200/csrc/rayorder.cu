@@ -97,21 +97,34 @@ __global__ void k_batch_fill_slots(const uint32_t* __restrict__ sorted, int64_t 
   slot_ray[views[v].slot_offset + (p - views[v].ray_offset)] = int32_t(sorted[p]);
 }
 
-// Key of forward slot s: its ray's consumed events (coarsened by `shift`), costliest first.
+// Key of forward slot s: its ray's consumed events (coarsened by `shift`), costliest first;
+// with views (batched slots), the slot's view above that, so each view's slots stay
+// together (a warp's lanes then replay rays of one view and one scene).
 __global__ void k_bwd_keys(const int32_t* __restrict__ iters, const int32_t* __restrict__ ray_order, int64_t R,
-                           int shift, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+                           int shift, const BatchView* __restrict__ views, int num_views, uint32_t* __restrict__ keys,
+                           uint32_t* __restrict__ vals) {
   const int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (s >= R) return;
   const int64_t r = ray_order ? int64_t(ray_order[s]) : s;
   const uint32_t n = r >= 0 ? uint32_t(max(iters[r], 0)) >> shift : 0u;  // padding slot: last
-  keys[s] = 255u - min(n, 255u);
+  uint32_t key = 255u - min(n, 255u);
+  if (views) {
+    int lo = 0, hi = num_views - 1;  // last view with slot_offset <= s
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (views[mid].slot_offset <= s) lo = mid;
+      else hi = mid - 1;
+    }
+    key |= uint32_t(lo) << 8;
+  }
+  keys[s] = key;
   vals[s] = uint32_t(s);
 }
 
 }  // namespace
 
 cudaError_t backward_slot_order(const int32_t* iters, const int32_t* ray_order, int64_t R, int shift, char* ws,
-                                int32_t* slot_order, cudaStream_t st) {
+                                int32_t* slot_order, cudaStream_t st, const BatchView* views, int num_views) {
   if (R == 0) return cudaSuccess;
   WsCursor c;
   uint32_t* ka = reinterpret_cast<uint32_t*>(ws + c.take(R * 4));
@@ -119,8 +132,8 @@ cudaError_t backward_slot_order(const int32_t* iters, const int32_t* ray_order, 
   uint32_t* kb = reinterpret_cast<uint32_t*>(ws + c.take(R * 4));
   uint32_t* vb = reinterpret_cast<uint32_t*>(ws + c.take(R * 4));
   uint32_t* hist = reinterpret_cast<uint32_t*>(ws + c.take((int64_t(sort_blocks(R)) * 256 + 512) * 4));
-  k_bwd_keys<<<unsigned((R + 255) / 256), 256, 0, st>>>(iters, ray_order, R, shift, ka, va);
-  sort_pairs(ka, va, kb, vb, hist, R, 8, st);
+  k_bwd_keys<<<unsigned((R + 255) / 256), 256, 0, st>>>(iters, ray_order, R, shift, views, num_views, ka, va);
+  sort_pairs(ka, va, kb, vb, hist, R, views ? 14 : 8, st);
   return cudaMemcpyAsync(slot_order, va, R * sizeof(int32_t), cudaMemcpyDeviceToDevice, st);
 }
 
