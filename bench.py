@@ -156,6 +156,30 @@ def cpu_baseline(sc, ro, rd, threads, target_s=10.0, n_rays=0):
     return n_rays / dt / 1e6, dt, n_rays
 
 
+def small_cpu_baselines(threads):
+    """The CPU paths on the small workload (1,000 uniform ellipsoids, SH0, one 64x64 view):
+    the reference's quadrature oracle as restated in numpy (2^16 samples per ray; a seeded
+    2-ray sample, single-threaded) and the exact CPU tracer's full forward (all threads)."""
+    from ever_b200 import synthetic as S
+    from oracle import oracle as O
+    from oracle import quad_np as Q
+    sc, cams = S.workload_small()
+    ro, rd = S.look_at_rays(cams[0])
+    idx = np.sort(np.random.default_rng(0).choice(ro.shape[0], 2, replace=False))
+    t0 = time.perf_counter()
+    Q.trace_rays(sc.mean, sc.scale, sc.quat, sc.density.reshape(-1), sc.features.reshape(-1, 3), ro[idx], rd[idx])
+    tq = time.perf_counter() - t0
+    s = O.Scene(sc.mean, sc.scale, sc.quat, sc.density.reshape(-1), sc.features)
+    O.trace(s, ro, rd, 0.0, 1000.0, 500, nthreads=threads)
+    t0 = time.perf_counter()
+    O.trace(s, ro, rd, 0.0, 1000.0, 500, nthreads=threads)
+    te = time.perf_counter() - t0
+    return {"quad_np": {"rays_per_s": 2 / tq, "cores": 1, "sample": "2 seeded rays of the 64x64 view",
+                        "full_view_s_extrapolated": ro.shape[0] * tq / 2},
+            "exact_cpu_forward": {"rays_per_s": ro.shape[0] / te, "cores": threads, "sample": "the full 64x64 view",
+                                  "ms": te * 1e3}}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -618,6 +642,7 @@ def main():
         v, dt, n = cpu_baseline(sc, ro, rd, threads, target_s=10.0, n_rays=args.cpu_sample)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"{n} seeded rays of the view, forward + FP64 backward, {dt:.1f} s"}
+        line["cpu_baselines_small"] = small_cpu_baselines(threads)
     if rank == 0 and world == 1 and not args.no_batched:
         line["batched"] = leg_batched(dev)
     if rank == 0 and world == 1 and not args.no_sched:
