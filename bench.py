@@ -610,9 +610,13 @@ def main():
     dom = "bwd" if ph["bwd"] >= ph["fwd"] else "fwd"
     b_dom = b_bwd if dom == "bwd" else b_fwd
     achieved = b_dom / (ph[dom] * 1e-3) / 1e9
+    # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one single-pass
+    # ncu capture of `bench.py --once` on this default workload (1M ellipsoids, 1920x1080)
+    measured_traffic = {"fwd": 221_817_600 + 378_326_528, "bwd": 2_844_346_112 + 400_863_488}
+    default_workload = args.prims == 1_000_000 and args.width == 1920 and args.height == 1080
     roofline = {"bound": "hbm", "kernel": "k_trace_bwd" if dom == "bwd" else "k_trace_fwd",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_kind": peak_kind, "traffic": None,
+                "peak_kind": peak_kind, "traffic": measured_traffic[dom] if default_workload else None,
                 "algorithmic_bytes": b_dom}
 
     line = {
