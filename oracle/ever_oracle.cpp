@@ -33,6 +33,7 @@
 #include <cstdint>
 #include <cstring>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 namespace {
@@ -449,8 +450,24 @@ int trace_impl(int64_t N, int Kc, int deg, const S* mean, const S* scale, const 
 // forward replay. FP32 with inverse_replay: the reference's own scheme
 // (backwards_kernel.slang:327-361): states recovered from the final state by
 // inverse_update_dual (spline-machine.slang:65-100), in float, as the CUDA kernel does.
+// Per-thread gradient accumulator, sparse over ellipsoids (a ray touches few of them):
+// one row per touched ellipsoid, W (9), mean (3), density (1), features (3 Kc).
 template <class T> struct Grad {
-  std::vector<T> W, mu, sigma, feat;  // per ellipsoid (W: 9 per ellipsoid)
+  int stride = 0;
+  std::unordered_map<int64_t, size_t> at;
+  std::vector<T> data;
+  T* row(int64_t p) {
+    auto it = at.find(p);
+    if (it != at.end()) return &data[it->second];
+    const size_t off = data.size();
+    data.resize(off + stride, T(0));
+    at.emplace(p, off);
+    return &data[off];
+  }
+  const T* find(int64_t p) const {
+    auto it = at.find(p);
+    return it == at.end() ? nullptr : &data[it->second];
+  }
 };
 
 // VJP of update() (T), cotangent G of the new state -> cotangent of the old
@@ -568,12 +585,7 @@ int backward_impl(int64_t N, int Kc, int deg, const double* mean, const double* 
   // per-thread accumulators to stay deterministic per thread; reduced at the end
   nthreads = std::max(1, (int)std::min<int64_t>(nthreads, std::max<int64_t>(R, 1)));
   std::vector<Grad<T>> acc(nthreads);
-  for (auto& g : acc) {
-    g.W.assign(9 * N, T(0));
-    g.mu.assign(3 * N, T(0));
-    g.sigma.assign(N, T(0));
-    g.feat.assign((size_t)N * Kc * 3, T(0));
-  }
+  for (auto& g : acc) g.stride = 13 + 3 * Kc;
   auto ray_fn = [&](int64_t j, Grad<T>& g) {
     double* gro = out.drayo + 3 * j;
     double* grd = out.drayd + 3 * j;
@@ -645,12 +657,13 @@ int backward_impl(int64_t N, int Kc, int deg, const double* mean, const double* 
       // dirac = dh * (1, c)
       T g_dh = Gdirac[0];
       for (int ch = 0; ch < 3; ++ch) g_dh += Gdirac[1 + ch] * cols[i][ch];
-      g.sigma[p] += sign * g_dh;
+      g.row(p)[12] += sign * g_dh;
       const T* f = &sc.feat[(size_t)p * Kc * 3];
+      T* gf = g.row(p) + 13;
       for (int ch = 0; ch < 3; ++ch) {
         const T gc = dh * Gdirac[1 + ch];
         for (int k = 0; k < nb; ++k) {
-          g.feat[(size_t)p * Kc * 3 + 3 * k + ch] += r.B[k] * gc;
+          gf[3 * k + ch] += r.B[k] * gc;
           G_B[k] += f[3 * k + ch] * gc;
         }
       }
@@ -679,11 +692,12 @@ int backward_impl(int64_t N, int Kc, int deg, const double* mean, const double* 
         }
         const T* Wp = &sc.W[9 * p];
         const T v[3] = {r.o[0] - sc.mu[3 * p], r.o[1] - sc.mu[3 * p + 1], r.o[2] - sc.mu[3 * p + 2]};
+        T* gr = g.row(p);
         for (int a = 0; a < 3; ++a)
           for (int b = 0; b < 3; ++b) {
-            g.W[9 * p + 3 * a + b] += g_ocn[a] * v[b] + g_rdn[a] * r.d[b];
+            gr[3 * a + b] += g_ocn[a] * v[b] + g_rdn[a] * r.d[b];
             const T wo = Wp[3 * a + b] * g_ocn[a];
-            g.mu[3 * p + b] -= wo;
+            gr[9 + b] -= wo;
             G_o[b] += wo;
             G_d[b] += Wp[3 * a + b] * g_rdn[a];
           }
@@ -697,12 +711,13 @@ int backward_impl(int64_t N, int Kc, int deg, const double* mean, const double* 
       const T sg = sc.sigma[p];
       T g_s = G.drgb[0];
       for (int ch = 0; ch < 3; ++ch) g_s += c[ch] * G.drgb[1 + ch];
-      g.sigma[p] += g_s;
+      g.row(p)[12] += g_s;
       const T* f = &sc.feat[(size_t)p * Kc * 3];
+      T* gf = g.row(p) + 13;
       for (int ch = 0; ch < 3; ++ch) {
         const T gc = sg * G.drgb[1 + ch];
         for (int k = 0; k < nb; ++k) {
-          g.feat[(size_t)p * Kc * 3 + 3 * k + ch] += r.B[k] * gc;
+          gf[3 * k + ch] += r.B[k] * gc;
           G_B[k] += f[3 * k + ch] * gc;
         }
       }
@@ -731,13 +746,27 @@ int backward_impl(int64_t N, int Kc, int deg, const double* mean, const double* 
       });
     for (auto& t : th) t.join();
   }
-  // reduce and convert W gradients to scale / quaternion gradients
-  for (int64_t p = 0; p < N; ++p) {
+  // reduce (threads in order) and convert W gradients to scale / quaternion gradients;
+  // ellipsoids no ray touched get zero gradients
+  std::fill(out.dmean, out.dmean + 3 * N, 0.0);
+  std::fill(out.dscale, out.dscale + 3 * N, 0.0);
+  std::fill(out.dquat, out.dquat + 4 * N, 0.0);
+  std::fill(out.ddensity, out.ddensity + N, 0.0);
+  std::fill(out.dfeat, out.dfeat + (size_t)N * Kc * 3, 0.0);
+  std::vector<int64_t> touched;
+  for (auto& g : acc)
+    for (const auto& kv : g.at) touched.push_back(kv.first);
+  std::sort(touched.begin(), touched.end());
+  touched.erase(std::unique(touched.begin(), touched.end()), touched.end());
+  std::vector<const T*> rows(acc.size());
+  for (int64_t p : touched) {
+    for (size_t k = 0; k < acc.size(); ++k) rows[k] = acc[k].find(p);
     T gW[9] = {0}, gmu[3] = {0}, gs = 0;
-    for (auto& g : acc) {
-      for (int i = 0; i < 9; ++i) gW[i] += g.W[9 * p + i];
-      for (int i = 0; i < 3; ++i) gmu[i] += g.mu[3 * p + i];
-      gs += g.sigma[p];
+    for (const T* gr : rows) {
+      if (!gr) continue;
+      for (int i = 0; i < 9; ++i) gW[i] += gr[i];
+      for (int i = 0; i < 3; ++i) gmu[i] += gr[9 + i];
+      gs += gr[12];
     }
     const T q[4] = {T(quat[4 * p]), T(quat[4 * p + 1]), T(quat[4 * p + 2]), T(quat[4 * p + 3])};
     const T s[3] = {T(scale[3 * p]), T(scale[3 * p + 1]), T(scale[3 * p + 2])};
@@ -760,7 +789,8 @@ int backward_impl(int64_t N, int Kc, int deg, const double* mean, const double* 
     out.ddensity[p] = gs;
     for (int i = 0; i < Kc * 3; ++i) {
       T v = 0;
-      for (auto& g : acc) v += g.feat[(size_t)p * Kc * 3 + i];
+      for (const T* gr : rows)
+        if (gr) v += gr[13 + i];
       out.dfeat[(size_t)p * Kc * 3 + i] = v;
     }
   }
