@@ -200,6 +200,7 @@ cudaError_t launch_log_to_reference(const int32_t* order, const int32_t* log, in
 constexpr int kOffW1 = 0, kOffW2 = 4096, kOffW3 = 8192, kOffB1 = 9216, kOffB2 = 9280, kOffB3 = 9344;
 constexpr int kMlpParams = 9360;
 constexpr int kMlpMaxGrid = 160;  // CTAs of a gradient launch (one partial-gradient slot each)
+constexpr int kMlpInferCtasPerSm = 6;  // resident inference CTAs per SM (64 TMEM columns each)
 
 struct MlpParams {
   const void* w1;  // bf16 [64 x 64]

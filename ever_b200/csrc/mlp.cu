@@ -14,6 +14,8 @@
 // products, which reduce over rays. Thread 0 issues the MMAs and tcgen05.commit signals
 // their completion on an mbarrier; every wait is bounded and reports a timeout through an
 // error flag instead of hanging.
+#include <cstddef>
+
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -28,8 +30,11 @@ constexpr int kHid = 64;
 constexpr int kOut = 16;    // padded output width (2 used)
 // tensor-memory columns: layer accumulators, then (training) weight-gradient accumulators
 constexpr uint32_t kColD1 = 0, kColD2 = 64, kColD3 = 128, kColGW1 = 256, kColGW2 = 320, kColGW3 = 384;
-constexpr uint32_t kColsInfer = 256, kColsTrain = 512;
+// inference: every layer's accumulator reuses D1's columns (each is read out before the next
+// MMA is issued), and one activation tile serves all three layers
+constexpr uint32_t kColsInfer = 64, kColsTrain = 512;
 constexpr size_t kTrainSmem = 120 * 1024;  // keeps one training CTA (512 TMEM columns) per SM
+constexpr int kInferCtasPerSm = kMlpInferCtasPerSm;  // 6 x 64 TMEM columns, about 37 KB shared memory each
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -108,19 +113,20 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 }
 
 struct Smem {
-  __nv_bfloat16 w1[kHid * kIn];    // [h1][in]  K-major, rows = output units
-  __nv_bfloat16 w2[kHid * kHid];   // [h2][h1]
-  __nv_bfloat16 w3[kOut * kHid];   // [out][h2]
-  __nv_bfloat16 a0[kTile * kIn];   // encoding           [ray][in]
+  float b1[kHid], b2[kHid], b3[kOut];
+  float gb1[4][kHid], gb2[4][kHid], gb3[4][kOut], loss[4];  // per-warp sums (fixed order)
+  uint64_t bar;
+  uint32_t tmem_base;
+  __align__(128) __nv_bfloat16 w1[kHid * kIn];  // [h1][in]  K-major, rows = output units
+  __nv_bfloat16 w2[kHid * kHid];                 // [h2][h1]
+  __nv_bfloat16 w3[kOut * kHid];                 // [out][h2]
+  __nv_bfloat16 a0[kTile * kIn];                 // encoding (inference: also hidden 1 and 2) [ray][in]
+  // training only: inference launches with the shared memory up to here
   __nv_bfloat16 a1[kTile * kHid];  // hidden 1            [ray][h1]
   __nv_bfloat16 a2[kTile * kHid];  // hidden 2            [ray][h2]
   __nv_bfloat16 g3[kTile * kOut];  // dL/d output         [ray][out]
   __nv_bfloat16 g2[kTile * kHid];  // dL/d pre-act 2      [ray][h2]
   __nv_bfloat16 g1[kTile * kHid];  // dL/d pre-act 1      [ray][h1]
-  float b1[kHid], b2[kHid], b3[kOut];
-  float gb1[4][kHid], gb2[4][kHid], gb3[4][kOut], loss[4];  // per-warp sums (fixed order)
-  uint64_t bar;
-  uint32_t tmem_base;
 };
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
@@ -167,25 +173,34 @@ __device__ __forceinline__ void encode(const MlpParams& P, int64_t r, float (&f)
   float x[3] = {(ox - od * dx) * P.inv_scale, (oy - od * dy) * P.inv_scale, (oz - od * dz) * P.inv_scale};
 #pragma unroll
   for (int i = 0; i < 3; ++i) x[i] = isfinite(x[i]) ? x[i] : 0.f;
-  int k = 0;
+  // sin / cos of 2^q pi x from one sincospi per component and the double-angle identities
+  // sin 2a = 2 sin a cos a, cos 2a = 1 - 2 sin^2 a (after five doublings the error is a
+  // few 1e-6, far below the bf16 rounding the features go through)
+  float sv[3], cv[3];
 #pragma unroll
-  for (int i = 0; i < 3; ++i) f[k++] = x[i];
-#pragma unroll
-  for (int q = 0; q < 6; ++q) {
-    const float s = float(1 << q);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) f[k++] = sinpif(s * x[i]);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) f[k++] = cospif(s * x[i]);
+  for (int i = 0; i < 3; ++i) {
+    f[i] = x[i];
+    sincospif(x[i], &sv[i], &cv[i]);
   }
 #pragma unroll
-  for (; k < kIn; ++k) f[k] = 0.f;
+  for (int q = 0; q < 6; ++q) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      f[3 + 6 * q + i] = sv[i];
+      f[6 + 6 * q + i] = cv[i];
+      const float s2 = 2.f * sv[i] * cv[i];
+      cv[i] = fmaf(-2.f * sv[i], sv[i], 1.f);
+      sv[i] = s2;
+    }
+  }
+#pragma unroll
+  for (int k = 39; k < kIn; ++k) f[k] = 0.f;
 }
 
 // Inference (TRAIN = false: predictions and cost bins) or the gradients of one training
 // batch (TRAIN = true: each CTA writes its partial gradient and loss to P.partial).
 template <bool TRAIN>
-__global__ void __launch_bounds__(128, 1) k_mlp(const MlpParams P) {
+__global__ void __launch_bounds__(128, TRAIN ? 1 : kInferCtasPerSm) k_mlp(const MlpParams P) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   Smem& S = *reinterpret_cast<Smem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -255,7 +270,12 @@ __global__ void __launch_bounds__(128, 1) k_mlp(const MlpParams P) {
     return __syncthreads_and(got) != 0;
   };
 
-  const uint32_t sa0 = smem_u32(S.a0), sa1 = smem_u32(S.a1), sa2 = smem_u32(S.a2);
+  // inference: hidden 1 and 2 overwrite the tile the previous (completed) MMA read
+  __nv_bfloat16* const a1 = TRAIN ? S.a1 : S.a0;
+  __nv_bfloat16* const a2 = TRAIN ? S.a2 : S.a0;
+  constexpr uint32_t kColH2 = TRAIN ? kColD2 : kColD1;  // inference: layers 2 and 3 reuse D1's columns
+  constexpr uint32_t kColY = TRAIN ? kColD3 : kColD1;
+  const uint32_t sa0 = smem_u32(S.a0), sa1 = smem_u32(a1), sa2 = smem_u32(a2);
   const uint32_t sw1 = smem_u32(S.w1), sw2 = smem_u32(S.w2), sw3 = smem_u32(S.w3);
   const uint32_t sg1 = smem_u32(S.g1), sg2 = smem_u32(S.g2), sg3 = smem_u32(S.g3);
   const int64_t ntiles = (P.num_samples + kTile - 1) / kTile;
@@ -285,32 +305,32 @@ __global__ void __launch_bounds__(128, 1) k_mlp(const MlpParams P) {
       tmem_ld16(tmem + lane_off + kColD1 + c0, v);
 #pragma unroll
       for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i] + S.b1[c0 + i], 0.f);
-      st8(S.a1, tid, c0, kTile, v);
-      st8(S.a1, tid, c0 + 8, kTile, v + 8);
+      st8(a1, tid, c0, kTile, v);
+      st8(a1, tid, c0 + 8, kTile, v + 8);
     }
     // layer 2: D2 = A1 W2^T
     ok = run([&] {
       for (int ks = 0; ks < kHid / 16; ++ks)
-        mma(tmem + kColD2, desc_k(sa1, kTile, ks), desc_k(sw2, kHid, ks), idesc(128, kHid, false, false), ks > 0);
+        mma(tmem + kColH2, desc_k(sa1, kTile, ks), desc_k(sw2, kHid, ks), idesc(128, kHid, false, false), ks > 0);
     });
     if (!ok) break;
 #pragma unroll
     for (int c0 = 0; c0 < kHid; c0 += 16) {
       float v[16];
-      tmem_ld16(tmem + lane_off + kColD2 + c0, v);
+      tmem_ld16(tmem + lane_off + kColH2 + c0, v);
 #pragma unroll
       for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i] + S.b2[c0 + i], 0.f);
-      st8(S.a2, tid, c0, kTile, v);
-      st8(S.a2, tid, c0 + 8, kTile, v + 8);
+      st8(a2, tid, c0, kTile, v);
+      st8(a2, tid, c0 + 8, kTile, v + 8);
     }
     // layer 3: D3[128 x 16] = A2 W3^T
     ok = run([&] {
       for (int ks = 0; ks < kHid / 16; ++ks)
-        mma(tmem + kColD3, desc_k(sa2, kTile, ks), desc_k(sw3, kOut, ks), idesc(128, kOut, false, false), ks > 0);
+        mma(tmem + kColY, desc_k(sa2, kTile, ks), desc_k(sw3, kOut, ks), idesc(128, kOut, false, false), ks > 0);
     });
     if (!ok) break;
     float y[16];
-    tmem_ld16(tmem + lane_off + kColD3, y);
+    tmem_ld16(tmem + lane_off + kColY, y);
     const float y0 = y[0] + S.b3[0], y1 = y[1] + S.b3[1];
     ++tiles_done;
     if (!TRAIN) {
@@ -489,13 +509,18 @@ static_assert(kOffW2 == kOffW1 + kHid * kIn && kOffW3 == kOffW2 + kHid * kHid &&
                   kOffB2 == kOffB1 + kHid && kOffB3 == kOffB2 + kHid && kMlpParams == kOffB3 + kOut,
               "parameter block layout");
 static_assert(sizeof(Smem) + 128 <= kTrainSmem, "training shared memory");
+constexpr size_t kInferSmem = offsetof(Smem, a1) + 128;
+static_assert(kInferCtasPerSm * (kInferSmem + 1024) <= 228 * 1024, "inference CTAs per SM");
+static_assert(kInferCtasPerSm * kColsInfer <= 512, "inference TMEM columns per SM");
+static_assert(offsetof(Smem, w1) % 128 == 0 && offsetof(Smem, a0) % 128 == 0 && offsetof(Smem, a1) % 128 == 0,
+              "tiles aligned");
 static_assert(kmaj(127, 63, 128) + 2 == kTile * kIn * 2, "tile layout covers the tile");
 
 }  // namespace
 
 cudaError_t launch_mlp(const MlpParams& P, bool train, int max_grid, cudaStream_t st) {
   if (P.num_samples == 0) return cudaSuccess;
-  const size_t smem = train ? kTrainSmem : sizeof(Smem) + 128;
+  const size_t smem = train ? kTrainSmem : kInferSmem;
   auto kern = train ? k_mlp<true> : k_mlp<false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;

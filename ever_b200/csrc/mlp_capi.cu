@@ -64,7 +64,7 @@ int ever_mlp_predict(const EverMlp* mlp, const float* rayo, const float* rayd, c
   if (bins)
     for (int i = 0; i < 3; ++i) P.thr[i] = thresholds[i];
   P.error = error;
-  return cuda_status(ever::launch_mlp(P, false, 2 * sm_count(), static_cast<cudaStream_t>(stream)),
+  return cuda_status(ever::launch_mlp(P, false, ever::kMlpInferCtasPerSm * sm_count(), static_cast<cudaStream_t>(stream)),
                      "ever_mlp_predict");
 }
 
