@@ -113,6 +113,19 @@ SIGNATURES = {
     "ever_sh_prepass": (ctypes.c_int, [c_p, c_p, c_i64, c_i32, c_i32, c_p, c_i32, c_p, c_p]),
     "ever_sh_prepass_backward": (ctypes.c_int, [c_p, c_p, c_i64, c_i32, c_i32, c_p, c_i32, c_p, c_p, c_p]),
     "ever_camera_rays": (ctypes.c_int, [ctypes.POINTER(EverCamera), c_p, c_p, c_p, c_p]),
+    "ever_camera_slots": (c_i64, [ctypes.POINTER(EverCamera)]),
+    "ever_camera_slot_pixels": (ctypes.c_int, [ctypes.POINTER(EverCamera), c_p, c_p]),
+    "ever_trace_forward_camera": (ctypes.c_int, [ctypes.POINTER(EverScene), ctypes.POINTER(EverCamera), c_p,
+                                                 ctypes.POINTER(EverTraceArgs), ctypes.POINTER(EverTune),
+                                                 ctypes.POINTER(EverForwardOut), c_p]),
+    "ever_trace_backward_camera": (ctypes.c_int, [ctypes.POINTER(EverScene), ctypes.POINTER(EverCamera), c_p,
+                                                  ctypes.POINTER(EverTraceArgs), c_p, c_p, c_p, c_p, c_i32, c_p,
+                                                  c_i32, c_p, c_p, c_p, c_p, c_sz, c_p, ctypes.POINTER(EverTune),
+                                                  ctypes.POINTER(EverBackwardOut), c_p]),
+    "ever_camera_backward_slot_order": (ctypes.c_int, [ctypes.POINTER(EverCamera), c_p, c_i32, c_p, c_sz, c_p,
+                                                       c_p]),
+    "ever_camera_event_log_to_reference": (ctypes.c_int, [ctypes.POINTER(EverScene), ctypes.POINTER(EverCamera),
+                                                          c_p, c_i32, c_p, c_p, c_i32, c_p]),
     "ever_ray_order_binned": (ctypes.c_int, [c_p, c_p, c_p, c_i64, c_p, c_sz, c_p, c_p]),
     "ever_batch_order_binned": (ctypes.c_int, [ctypes.POINTER(EverBatch), c_p, c_p, c_p, c_p]),
 }

@@ -4,6 +4,7 @@
 #include <cstring>
 #include <string>
 
+#include "camera.cuh"
 #include "common.cuh"
 #include "internal.cuh"
 
@@ -151,11 +152,15 @@ int trace_backward(const EverScene* scene, const float* rayo, const float* rayd,
                    const int32_t* event_log, int32_t log_cap, const float* wct, int32_t num_wct, const float* mean,
                    const float* scale, const float* quat, void* workspace, size_t workspace_bytes,
                    const int32_t* ray_order, const int32_t* slot_order, const EverTune* tune,
-                   const EverBackwardOut* out, void* stream) {
+                   const EverBackwardOut* out, void* stream, const ever::CameraParams* cam = nullptr,
+                   const float* jitter = nullptr) {
   if (!scene || !args || !out) return fail(EVER_ERR_INVALID, "null scene, args or out");
   const int64_t N = scene->num_prims;
   if (num_rays < 0) return fail(EVER_ERR_INVALID, "num_rays out of range");
-  if (num_rays > 0 && (!rayo || !rayd || !grad_out || !states || !iters || !event_log || !out->drayo || !out->drayd))
+  // camera traces make their rays in the kernels and may skip the ray gradients
+  const bool need_rays = !cam, need_dray = !cam || out->drayo || out->drayd;
+  if (num_rays > 0 && ((need_rays && (!rayo || !rayd)) || !grad_out || !states || !iters || !event_log ||
+                       (need_dray && (!out->drayo || !out->drayd))))
     return fail(EVER_ERR_INVALID, "null ray-side pointer");
   if (N > 0 && (!mean || !scale || !quat || !out->dmean || !out->dscale || !out->dquat || !out->ddensity ||
                 !out->dfeatures))
@@ -193,7 +198,7 @@ int trace_backward(const EverScene* scene, const float* rayo, const float* rayd,
     P.K = scene->sh_coeffs;
     P.rayo = rayo;
     P.rayd = rayd;
-    P.R = num_rays;
+    P.R = cam ? ever::camera_slots(*cam) : num_rays;  // threads, and the event-log row length
     P.tmin = args->tmin;
     P.tmax = args->tmax;
     P.max_iters = args->max_iters;
@@ -211,7 +216,7 @@ int trace_backward(const EverScene* scene, const float* rayo, const float* rayd,
     P.dmeans2d = out->dmeans2d;
     P.drayo = out->drayo;
     P.drayd = out->drayd;
-    e = ever::launch_backward(P, deg, tn, st);
+    e = cam ? ever::launch_backward_camera(P, *cam, jitter, deg, tn, st) : ever::launch_backward(P, deg, tn, st);
     if (e != cudaSuccess) return cuda_status(e, "ever_trace_backward");
     ever::FinalizeParams F{};
     F.records = scene->records;
@@ -230,7 +235,7 @@ int trace_backward(const EverScene* scene, const float* rayo, const float* rayd,
     return cuda_status(e, "ever_trace_backward finalize");
   }
   // no ellipsoids: every ray gradient is zero
-  if (num_rays > 0) {
+  if (num_rays > 0 && out->drayo) {
     e = cudaMemsetAsync(out->drayo, 0, num_rays * 3 * sizeof(float), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(out->drayd, 0, num_rays * 3 * sizeof(float), st);
   }
@@ -302,6 +307,99 @@ int ever_ray_order(const float* rayo, const float* rayd, int64_t num_rays, void*
   return cuda_status(ever::ray_order(rayo, rayd, num_rays, static_cast<char*>(workspace), ray_order,
                                      static_cast<cudaStream_t>(stream)),
                      "ever_ray_order");
+}
+
+// ---- camera traces: rays made from the camera inside the kernels ----
+
+int64_t ever_camera_slots(const EverCamera* camera) {
+  ever::CameraParams C{};
+  if (const char* msg = ever::camera_params(camera, &C)) {
+    fail(EVER_ERR_INVALID, "ever_camera_slots: %s", msg);
+    return -1;
+  }
+  return ever::camera_slots(C);
+}
+
+int ever_camera_slot_pixels(const EverCamera* camera, int32_t* slot_pixel, void* stream) {
+  ever::CameraParams C{};
+  if (const char* msg = ever::camera_params(camera, &C))
+    return fail(EVER_ERR_INVALID, "ever_camera_slot_pixels: %s", msg);
+  if (ever::camera_slots(C) > 0 && !slot_pixel) return fail(EVER_ERR_INVALID, "ever_camera_slot_pixels: null output");
+  return cuda_status(ever::launch_camera_slot_pixels(C, slot_pixel, static_cast<cudaStream_t>(stream)),
+                     "ever_camera_slot_pixels");
+}
+
+int ever_trace_forward_camera(const EverScene* scene, const EverCamera* camera, const float* jitter,
+                              const EverTraceArgs* args, const EverTune* tune, const EverForwardOut* out,
+                              void* stream) {
+  if (!scene || !args || !out) return fail(EVER_ERR_INVALID, "null scene, args or out");
+  ever::CameraParams C{};
+  if (const char* msg = ever::camera_params(camera, &C))
+    return fail(EVER_ERR_INVALID, "ever_trace_forward_camera: %s", msg);
+  const int64_t R = int64_t(C.width) * C.height;
+  if (R > 0 && (!out->out || !out->iters)) return fail(EVER_ERR_INVALID, "null out or iters");
+  if (out->event_log && out->log_cap < 0) return fail(EVER_ERR_INVALID, "negative log_cap");
+  int deg = 0;
+  if (int rc = resolve_degree(scene, args, &deg)) return rc;
+  ever::FwdParams P{};
+  P.nodes = scene->nodes;
+  P.records = scene->records;
+  P.features = scene->features;
+  P.order = scene->order;
+  P.N = scene->num_prims;
+  P.K = scene->sh_coeffs;
+  P.R = R;
+  P.tmin = args->tmin;
+  P.tmax = args->tmax;
+  P.max_iters = args->max_iters;
+  P.out = *out;
+  return cuda_status(
+      ever::launch_forward_camera(P, C, jitter, deg, resolve_tune(tune), static_cast<cudaStream_t>(stream)),
+      "ever_trace_forward_camera");
+}
+
+int ever_trace_backward_camera(const EverScene* scene, const EverCamera* camera, const float* jitter,
+                               const EverTraceArgs* args, const float* grad_out, const float* states,
+                               const int32_t* iters, const int32_t* event_log, int32_t log_cap, const float* wct,
+                               int32_t num_wct, const float* mean, const float* scale, const float* quat,
+                               void* workspace, size_t workspace_bytes, const int32_t* slot_order,
+                               const EverTune* tune, const EverBackwardOut* out, void* stream) {
+  ever::CameraParams C{};
+  if (const char* msg = ever::camera_params(camera, &C))
+    return fail(EVER_ERR_INVALID, "ever_trace_backward_camera: %s", msg);
+  return trace_backward(scene, nullptr, nullptr, int64_t(C.width) * C.height, args, grad_out, states, iters,
+                        event_log, log_cap, wct, num_wct, mean, scale, quat, workspace, workspace_bytes, nullptr,
+                        slot_order, tune, out, stream, &C, jitter);
+}
+
+int ever_camera_backward_slot_order(const EverCamera* camera, const int32_t* iters, int32_t shift, void* workspace,
+                                    size_t workspace_bytes, int32_t* slot_order, void* stream) {
+  ever::CameraParams C{};
+  if (const char* msg = ever::camera_params(camera, &C))
+    return fail(EVER_ERR_INVALID, "ever_camera_backward_slot_order: %s", msg);
+  if (shift < 0 || shift > 16) return fail(EVER_ERR_INVALID, "shift %d out of range 0..16", shift);
+  const int64_t S = ever::camera_slots(C);
+  if (S > 0 && (!iters || !slot_order)) return fail(EVER_ERR_INVALID, "null pointer");
+  const int64_t need = ever::ray_order_workspace(S);
+  if (S > 0 && (!workspace || workspace_bytes < size_t(need)))
+    return fail(EVER_ERR_WORKSPACE, "slot order workspace needs %lld bytes, got %zu", (long long)need,
+                workspace_bytes);
+  return cuda_status(ever::camera_backward_slot_order(C, iters, shift, static_cast<char*>(workspace), slot_order,
+                                                      static_cast<cudaStream_t>(stream)),
+                     "ever_camera_backward_slot_order");
+}
+
+int ever_camera_event_log_to_reference(const EverScene* scene, const EverCamera* camera, const int32_t* event_log,
+                                       int32_t log_cap, const int32_t* iters, int32_t* tri_collection,
+                                       int32_t max_iters, void* stream) {
+  ever::CameraParams C{};
+  if (const char* msg = ever::camera_params(camera, &C))
+    return fail(EVER_ERR_INVALID, "ever_camera_event_log_to_reference: %s", msg);
+  if (!scene || (int64_t(C.width) * C.height > 0 && max_iters > 0 && (!event_log || !iters || !tri_collection)))
+    return fail(EVER_ERR_INVALID, "null pointer");
+  return cuda_status(ever::launch_camera_log_to_reference(C, scene->order, event_log, log_cap, iters, tri_collection,
+                                                          max_iters, static_cast<cudaStream_t>(stream)),
+                     "ever_camera_event_log_to_reference");
 }
 
 }  // extern "C"

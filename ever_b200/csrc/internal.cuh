@@ -243,4 +243,21 @@ struct CameraParams {
 };
 cudaError_t launch_camera_rays(const CameraParams& C, const float* jitter, float* rayo, float* rayd, cudaStream_t st);
 
+// Camera traces (rays made in the kernels; slots of 8x4 pixel tiles, camera.cuh).
+cudaError_t launch_forward_camera(const FwdParams& P, const CameraParams& cam, const float* jitter, int deg,
+                                  const EverTune& tune, cudaStream_t st);
+template <int KBUF>
+cudaError_t launch_forward_camera_k(const FwdParams& P, const CameraParams& cam, const float* jitter, int deg,
+                                    int block, cudaStream_t st);
+// Backward of a camera trace: P.R is the slot count, P.slot_order (nullable) the launch
+// order over slots, P.ray_order unused; drayo/drayd (nullable) are indexed by pixel.
+cudaError_t launch_backward_camera(const BwdParams& P, const CameraParams& cam, const float* jitter, int deg,
+                                   const EverTune& tune, cudaStream_t st);
+cudaError_t camera_backward_slot_order(const CameraParams& cam, const int32_t* iters, int shift, char* ws,
+                                       int32_t* slot_order, cudaStream_t st);
+cudaError_t launch_camera_slot_pixels(const CameraParams& cam, int32_t* slot_pixel, cudaStream_t st);
+cudaError_t launch_camera_log_to_reference(const CameraParams& cam, const int32_t* order, const int32_t* log,
+                                           int log_cap, const int32_t* iters, int32_t* tri, int max_iters,
+                                           cudaStream_t st);
+
 }  // namespace ever

@@ -15,6 +15,9 @@
 // rayd = R d, rayo = camera centre, where [R | t] is the camera-to-world matrix; the
 // offsets (ox, oy) are 0.5 (pixel centres) or given per pixel (the trainer's random
 // jitter). Rays are row-major over the image.
+#include <string>
+
+#include "camera.cuh"
 #include "common.cuh"
 #include "internal.cuh"
 
@@ -85,17 +88,14 @@ __global__ void k_camera_rays(CameraParams C, const float* __restrict__ jitter, 
   const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t R = int64_t(C.width) * C.height;
   if (p >= R) return;
-  const int row = int(p / C.width), col = int(p - int64_t(row) * C.width);
-  const float ox = jitter ? jitter[2 * p] : 0.5f, oy = jitter ? jitter[2 * p + 1] : 0.5f;
-  const float x = ((float(col) + ox) - C.cx) / C.fx;
-  const float y = ((float(row) + oy) - C.cy) / C.fy;
-  const float n = sqrtf(x * x + y * y + 1.f);
-  const float d[3] = {x / n, y / n, 1.f / n};
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    rayd[3 * p + a] = C.c2w[4 * a] * d[0] + C.c2w[4 * a + 1] * d[1] + C.c2w[4 * a + 2] * d[2];
-    rayo[3 * p + a] = C.c2w[4 * a + 3];
-  }
+  float3 o, d;
+  camera_ray(C, jitter, p, o, d);
+  rayo[3 * p] = o.x;
+  rayo[3 * p + 1] = o.y;
+  rayo[3 * p + 2] = o.z;
+  rayd[3 * p] = d.x;
+  rayd[3 * p + 1] = d.y;
+  rayd[3 * p + 2] = d.z;
 }
 
 template <int DEG>
@@ -162,21 +162,11 @@ int ever_sh_prepass_backward(const float* mean, const float* features, int64_t n
 }
 
 int ever_camera_rays(const EverCamera* camera, const float* jitter, float* rayo, float* rayd, void* stream) {
-  if (!camera) return ever::set_last_error(EVER_ERR_INVALID, "ever_camera_rays: null camera");
-  if (camera->width < 0 || camera->height < 0 || int64_t(camera->width) * camera->height >= (int64_t(1) << 31))
-    return ever::set_last_error(EVER_ERR_INVALID, "ever_camera_rays: image size out of range");
-  if (!(camera->fx != 0.f) || !(camera->fy != 0.f))
-    return ever::set_last_error(EVER_ERR_INVALID, "ever_camera_rays: zero focal length");
-  if (int64_t(camera->width) * camera->height > 0 && (!rayo || !rayd))
-    return ever::set_last_error(EVER_ERR_INVALID, "ever_camera_rays: null output");
   ever::CameraParams C{};
-  C.width = camera->width;
-  C.height = camera->height;
-  C.fx = camera->fx;
-  C.fy = camera->fy;
-  C.cx = camera->cx;
-  C.cy = camera->cy;
-  for (int i = 0; i < 12; ++i) C.c2w[i] = camera->c2w[i];
+  if (const char* msg = ever::camera_params(camera, &C))
+    return ever::set_last_error(EVER_ERR_INVALID, (std::string("ever_camera_rays: ") + msg).c_str());
+  if (int64_t(C.width) * C.height > 0 && (!rayo || !rayd))
+    return ever::set_last_error(EVER_ERR_INVALID, "ever_camera_rays: null output");
   const cudaError_t e = ever::launch_camera_rays(C, jitter, rayo, rayd, static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? EVER_OK : ever::set_last_error(EVER_ERR_CUDA, cudaGetErrorString(e));
 }

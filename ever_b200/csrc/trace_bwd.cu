@@ -8,6 +8,7 @@
 // of |ocn + t rdn|^2 = 1 and of the SH colour. Gradients of the 3x3 local-frame matrix W
 // are accumulated per ellipsoid and turned into scale/quaternion gradients once per
 // ellipsoid by k_finalize.
+#include "camera.cuh"
 #include "common.cuh"
 #include "internal.cuh"
 
@@ -283,21 +284,27 @@ __device__ __forceinline__ float colour_grads(const BScene& P, int j, float dh, 
   return sign * g_dh;
 }
 
-// Reverse replay of ray r (event-log column `slot`) against scene S.
+__device__ __forceinline__ float3 load3(const float* v, int64_t r) {
+  return make_float3(v[3 * r], v[3 * r + 1], v[3 * r + 2]);
+}
+
+// Reverse replay of ray r = (ro, rd) (event-log column `slot`) against scene S. Ray
+// gradients are written to P.drayo / P.drayd row r unless those are null.
 template <int DEG>
-__device__ void backward_ray(const BScene& S, const BRayCtx& P, int64_t r, int64_t slot, int* st_node, int stride) {
+__device__ void backward_ray(const BScene& S, const BRayCtx& P, int64_t r, int64_t slot, float3 ro, float3 rd,
+                             int* st_node, int stride) {
   const int n = P.iters[r];
-  float* gro = P.drayo + 3 * r;
-  float* grd = P.drayd + 3 * r;
   if (n >= P.max_iters - 1 || n <= 0) {  // backwards_kernel.slang:304
-    gro[0] = gro[1] = gro[2] = 0.f;
-    grd[0] = grd[1] = grd[2] = 0.f;
+    if (P.drayo) {
+      float* gro = P.drayo + 3 * r;
+      float* grd = P.drayd + 3 * r;
+      gro[0] = gro[1] = gro[2] = 0.f;
+      grd[0] = grd[1] = grd[2] = 0.f;
+    }
     return;
   }
   const Node* nodes = S.nodes;
   const Record* recs = S.recs;
-  const float3 ro = make_float3(P.rayo[3 * r], P.rayo[3 * r + 1], P.rayo[3 * r + 2]);
-  const float3 rd = make_float3(P.rayd[3 * r], P.rayd[3 * r + 1], P.rayd[3 * r + 2]);
   const Ray ray = make_ray(ro, rd, P.tmin);
   float B[16];
   sh_basis<DEG>(ray.rd, B);
@@ -467,6 +474,9 @@ __device__ void backward_ray(const BScene& S, const BRayCtx& P, int64_t r, int64
   }
 
   // ray gradients: o = rayo + tmin rayd; d = rayd / |rayd|; SH basis of the raw rayd
+  if (!P.drayo) return;
+  float* gro = P.drayo + 3 * r;
+  float* grd = P.drayd + 3 * r;
   float3 g_rd = sh_basis_vjp<DEG>(ray.rd, GB);
   const float dd = fmaf(rd.z, rd.z, fmaf(rd.y, rd.y, rd.x * rd.x));
   const float nrm = sqrtf(fmaxf(dd, kTiny));
@@ -494,7 +504,28 @@ __global__ void __launch_bounds__(256) k_trace_bwd(const BwdParams P) {
                  P.acc_geo, P.acc_feat};
   const BRayCtx C{P.rayo, P.rayd, P.tmin, P.max_iters, P.grad_out, P.states, P.iters, P.event_log, P.R,
                   P.drayo, P.drayd, P.wct, P.num_wct, P.dmeans2d};
-  backward_ray<DEG>(S, C, r, slot, smem + tid, blockDim.x);
+  backward_ray<DEG>(S, C, r, slot, load3(P.rayo, r), load3(P.rayd, r), smem + tid, blockDim.x);
+}
+
+// Backward of a camera trace: threads take slots (through the slot order, if any), make
+// the slot's pixel ray from the camera as the forward did, and replay it.
+template <int DEG>
+__global__ void __launch_bounds__(256)
+    k_trace_bwd_camera(const BwdParams P, const CameraParams cam, const float* __restrict__ jitter) {
+  extern __shared__ int smem[];
+  const int tid = threadIdx.x;
+  const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;
+  if (gi >= P.R) return;
+  const int64_t slot = P.slot_order ? int64_t(P.slot_order[gi]) : gi;
+  const int64_t p = camera_slot_pixel(cam, slot);
+  if (p < 0) return;
+  const BScene S{reinterpret_cast<const Node*>(P.nodes), reinterpret_cast<const Record*>(P.records), P.features, P.K,
+                 P.acc_geo, P.acc_feat};
+  const BRayCtx C{nullptr, nullptr, P.tmin, P.max_iters, P.grad_out, P.states, P.iters, P.event_log, P.R,
+                  P.drayo, P.drayd, P.wct, P.num_wct, P.dmeans2d};
+  float3 ro, rd;
+  camera_ray(cam, jitter, p, ro, rd);
+  backward_ray<DEG>(S, C, p, slot, ro, rd, smem + tid, blockDim.x);
 }
 
 // Persistent batched backward: warps take 32-slot packets from a device counter. With a
@@ -526,7 +557,7 @@ __global__ void __launch_bounds__(256) k_trace_bwd_batched(const BatchBwdParams 
     const BScene S{reinterpret_cast<const Node*>(bs_.nodes), reinterpret_cast<const Record*>(bs_.records),
                    bs_.features, bs_.K, bs_.acc_geo, bs_.acc_feat};
     const int32_t r = P.slot_ray[slot];
-    if (r >= 0) backward_ray<DEG>(S, C, r, slot, smem + tid, blockDim.x);
+    if (r >= 0) backward_ray<DEG>(S, C, r, slot, load3(P.rayo, r), load3(P.rayd, r), smem + tid, blockDim.x);
     __syncwarp();
   }
 }
@@ -630,6 +661,39 @@ cudaError_t launch_b(const BwdParams& P, int block, cudaStream_t st) {
 }  // namespace
 
 template <int DEG>
+cudaError_t launch_bc(const BwdParams& P, const CameraParams& cam, const float* jitter, int block, cudaStream_t st) {
+  const size_t smem = size_t(kStackDepth) * block * sizeof(int);
+  auto kern = k_trace_bwd_camera<DEG>;
+  cudaError_t e = cudaSuccess;
+  if (smem > 48 * 1024) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  kern<<<unsigned((P.R + block - 1) / block), block, smem, st>>>(P, cam, jitter);
+  return cudaGetLastError();
+}
+
+__global__ void k_camera_slot_pixels(const CameraParams cam, int64_t num_slots, int32_t* __restrict__ slot_pixel) {
+  const int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (s < num_slots) slot_pixel[s] = int32_t(camera_slot_pixel(cam, s));
+}
+
+__global__ void k_camera_log_to_reference(const CameraParams cam, int64_t num_slots, const int32_t* __restrict__ order,
+                                          const int32_t* __restrict__ log, int log_cap,
+                                          const int32_t* __restrict__ iters, int32_t* __restrict__ tri,
+                                          int max_iters) {
+  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= num_slots * int64_t(max_iters)) return;
+  const int64_t i = t / num_slots, slot = t - i * num_slots;
+  const int64_t r = camera_slot_pixel(cam, slot);
+  if (r < 0) return;
+  int32_t v = 0;
+  if (i < iters[r] && i < log_cap) {
+    const int32_t id = log[i * num_slots + slot];
+    v = 2 * order[id >> 1] + (id & 1);
+  }
+  tri[i * (int64_t(cam.width) * cam.height) + r] = v;
+}
+
+template <int DEG>
 cudaError_t launch_bb(const BatchBwdParams& P, int block, cudaStream_t st) {
   const size_t smem = size_t(kStackDepth) * block * sizeof(int);
   auto kern = k_trace_bwd_batched<DEG>;
@@ -662,6 +726,35 @@ cudaError_t launch_backward(const BwdParams& P, int deg, const EverTune& tune, c
     case 2: return launch_b<2>(P, block, st);
     default: return launch_b<3>(P, block, st);
   }
+}
+
+cudaError_t launch_backward_camera(const BwdParams& P, const CameraParams& cam, const float* jitter, int deg,
+                                   const EverTune& tune, cudaStream_t st) {
+  if (P.R == 0) return cudaSuccess;
+  const int block = tune.block > 0 ? tune.block : 128;
+  switch (deg) {
+    case 0: return launch_bc<0>(P, cam, jitter, block, st);
+    case 1: return launch_bc<1>(P, cam, jitter, block, st);
+    case 2: return launch_bc<2>(P, cam, jitter, block, st);
+    default: return launch_bc<3>(P, cam, jitter, block, st);
+  }
+}
+
+cudaError_t launch_camera_slot_pixels(const CameraParams& cam, int32_t* slot_pixel, cudaStream_t st) {
+  const int64_t n = camera_slots(cam);
+  if (n == 0) return cudaSuccess;
+  k_camera_slot_pixels<<<unsigned((n + 255) / 256), 256, 0, st>>>(cam, n, slot_pixel);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_camera_log_to_reference(const CameraParams& cam, const int32_t* order, const int32_t* log,
+                                           int log_cap, const int32_t* iters, int32_t* tri, int max_iters,
+                                           cudaStream_t st) {
+  const int64_t n = camera_slots(cam) * int64_t(max_iters);
+  if (n == 0) return cudaSuccess;
+  k_camera_log_to_reference<<<unsigned((n + 255) / 256), 256, 0, st>>>(cam, camera_slots(cam), order, log, log_cap,
+                                                                       iters, tri, max_iters);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_finalize(const FinalizeParams& P, cudaStream_t st) {

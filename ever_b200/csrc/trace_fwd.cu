@@ -25,4 +25,15 @@ cudaError_t launch_forward(const FwdParams& P, int deg, const EverTune& tune, cu
   }
 }
 
+cudaError_t launch_forward_camera(const FwdParams& P, const CameraParams& cam, const float* jitter, int deg,
+                                  const EverTune& tune, cudaStream_t st) {
+  if (int64_t(cam.width) * cam.height == 0) return cudaSuccess;
+  const int block = tune.block > 0 ? tune.block : 128;
+  switch (tune.kbuf) {
+    case 8: return launch_forward_camera_k<8>(P, cam, jitter, deg, block, st);
+    case 32: return launch_forward_camera_k<32>(P, cam, jitter, deg, block, st);
+    default: return launch_forward_camera_k<16>(P, cam, jitter, deg, block, st);
+  }
+}
+
 }  // namespace ever

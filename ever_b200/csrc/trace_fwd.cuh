@@ -21,6 +21,7 @@
 // inside the reference round that consumed its entry. The result is the reference's
 // event sequence for any KBUF.
 #pragma once
+#include "camera.cuh"
 #include "common.cuh"
 #include "internal.cuh"
 
@@ -440,10 +441,8 @@ __global__ void __launch_bounds__(256) k_trace_fwd_ray(const FwdParams P) {
 // One warp traces one packet of up to 32 rays against one scene (lanes with valid=false
 // only take part in the warp-wide votes).
 template <int KBUF, int DEG>
-__device__ __forceinline__ void trace_packet(const SceneRef& sc, const TraceCtx& C, const float* rayo,
-                                             const float* rayd, int64_t r, bool valid, int64_t slot, int* wstack,
-                                             float* B, int bs, int lane) {
-  const Ray ray = load_ray(rayo, rayd, valid ? r : 0, C.tmin);
+__device__ __forceinline__ void trace_packet(const SceneRef& sc, const TraceCtx& C, const Ray& ray, int64_t r,
+                                             bool valid, int64_t slot, int* wstack, float* B, int bs, int lane) {
   const RaySlab sl = make_slab(ray);
   {
     float Bl[16];
@@ -495,7 +494,29 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value) k_trace_fwd
   const bool valid = gi < P.R;  // every lane stays for the warp-wide ballots
   const int64_t r = valid ? (P.ray_order ? int64_t(P.ray_order[gi]) : gi) : 0;
   const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out};
-  trace_packet<KBUF, DEG>(scene_of(P), C, P.rayo, P.rayd, r, valid, gi, wstack, B, blockDim.x, lane);
+  const Ray ray = load_ray(P.rayo, P.rayd, r, P.tmin);
+  trace_packet<KBUF, DEG>(scene_of(P), C, ray, r, valid, gi, wstack, B, blockDim.x, lane);
+}
+
+// Camera trace: rays are made from the camera in the kernel (no ray arrays). The launch
+// covers the camera's slots, 32 per 8x4 pixel tile, so a warp traces one tile; outputs are
+// written by pixel, event-log columns are slots.
+template <int KBUF, int DEG, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value)
+    k_trace_fwd_camera(const FwdParams P, const CameraParams cam, const float* __restrict__ jitter,
+                       int64_t num_slots) {
+  extern __shared__ int smem[];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int* wstack = smem + warp * kStackDepth;
+  float* B = reinterpret_cast<float*>(smem + (blockDim.x / 32) * kStackDepth) + tid;
+  const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;
+  const int64_t p = gi < num_slots ? camera_slot_pixel(cam, gi) : -1;
+  const bool valid = p >= 0;
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, num_slots, P.out};
+  float3 ro, rd;
+  camera_ray(cam, jitter, valid ? p : 0, ro, rd);
+  const Ray ray = make_ray(ro, rd, P.tmin);
+  trace_packet<KBUF, DEG>(scene_of(P), C, ray, valid ? p : 0, valid, gi, wstack, B, blockDim.x, lane);
 }
 
 // Persistent batched forward: warps take 32-slot packets from a device counter until
@@ -520,7 +541,8 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value) k_trace_fwd
     const SceneRef sc{reinterpret_cast<const Node*>(bs_.nodes), reinterpret_cast<const Record*>(bs_.records),
                       bs_.features, bs_.N, bs_.K};
     const int32_t r = P.slot_ray[slot];
-    trace_packet<KBUF, DEG>(sc, C, P.rayo, P.rayd, r, r >= 0, slot, wstack, B, blockDim.x, lane);
+    const Ray ray = load_ray(P.rayo, P.rayd, r >= 0 ? r : 0, P.tmin);
+    trace_packet<KBUF, DEG>(sc, C, ray, r, r >= 0, slot, wstack, B, blockDim.x, lane);
   }
 }
 
@@ -551,6 +573,31 @@ cudaError_t launch_k(const FwdParams& P, int deg, int block, int traversal, cuda
     case 1: return launch_t<KBUF, 1>(P, block, traversal, st);
     case 2: return launch_t<KBUF, 2>(P, block, traversal, st);
     default: return launch_t<KBUF, 3>(P, block, traversal, st);
+  }
+}
+
+template <int KBUF, int DEG>
+cudaError_t launch_camera_t(const FwdParams& P, const CameraParams& cam, const float* jitter, int block,
+                            cudaStream_t st) {
+  const int64_t num_slots = camera_slots(cam);
+  const unsigned grid = unsigned((num_slots + block - 1) / block);
+  const size_t smem = size_t(kStackDepth) * (block / 32) * sizeof(int) + size_t(16) * block * sizeof(float);
+  switch (block) {
+    case 64: k_trace_fwd_camera<KBUF, DEG, 64><<<grid, 64, smem, st>>>(P, cam, jitter, num_slots); break;
+    case 128: k_trace_fwd_camera<KBUF, DEG, 128><<<grid, 128, smem, st>>>(P, cam, jitter, num_slots); break;
+    default: k_trace_fwd_camera<KBUF, DEG, 256><<<grid, 256, smem, st>>>(P, cam, jitter, num_slots); break;
+  }
+  return cudaGetLastError();
+}
+
+template <int KBUF>
+cudaError_t launch_camera_k(const FwdParams& P, const CameraParams& cam, const float* jitter, int deg, int block,
+                            cudaStream_t st) {
+  switch (deg) {
+    case 0: return launch_camera_t<KBUF, 0>(P, cam, jitter, block, st);
+    case 1: return launch_camera_t<KBUF, 1>(P, cam, jitter, block, st);
+    case 2: return launch_camera_t<KBUF, 2>(P, cam, jitter, block, st);
+    default: return launch_camera_t<KBUF, 3>(P, cam, jitter, block, st);
   }
 }
 

@@ -9,6 +9,12 @@ cudaError_t launch_forward_k<32>(const FwdParams& P, int deg, int block, int tra
 }
 
 template <>
+cudaError_t launch_forward_camera_k<32>(const FwdParams& P, const CameraParams& cam, const float* jitter, int deg,
+                                         int block, cudaStream_t st) {
+  return launch_camera_k<32>(P, cam, jitter, deg, block, st);
+}
+
+template <>
 cudaError_t launch_forward_batched_k<32>(const BatchFwdParams& P, int deg, int block, cudaStream_t st) {
   return launch_batched_k<32>(P, deg, block, st);
 }

@@ -9,6 +9,12 @@ cudaError_t launch_forward_k<8>(const FwdParams& P, int deg, int block, int trav
 }
 
 template <>
+cudaError_t launch_forward_camera_k<8>(const FwdParams& P, const CameraParams& cam, const float* jitter, int deg,
+                                         int block, cudaStream_t st) {
+  return launch_camera_k<8>(P, cam, jitter, deg, block, st);
+}
+
+template <>
 cudaError_t launch_forward_batched_k<8>(const BatchFwdParams& P, int deg, int block, cudaStream_t st) {
   return launch_batched_k<8>(P, deg, block, st);
 }

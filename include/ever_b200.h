@@ -181,8 +181,8 @@ int ever_event_log_to_reference(const EverScene* scene, const int32_t* event_log
 size_t ever_ray_order_workspace_bytes(int64_t num_rays);
 
 /* A coherent launch order for R rays (no counterpart in the reference, whose OptiX
- * launch order is the ray index): rays sorted by a coarse origin cell and the Morton
- * code of their octahedral direction, so each warp's packet covers a compact patch.
+ * launch order is the ray index): rays sorted by a coarse origin cell and the Hilbert
+ * index of their octahedral direction, so each warp's packet covers a compact patch.
  * Writes a permutation of 0..R-1 to ray_order (R). Pass it to forward and backward. */
 int ever_ray_order(const float* rayo, const float* rayd, int64_t num_rays, void* workspace,
                    size_t workspace_bytes, int32_t* ray_order, void* stream);
@@ -364,6 +364,50 @@ typedef struct EverCamera {
  * per-pixel offsets (ox, oy); NULL means pixel centres (0.5, 0.5). Counterpart of
  * camera2rays / get_ray_directions / get_rays (integration_utils/gaussian_renderer/ever.py:29-74,105-118). */
 int ever_camera_rays(const EverCamera* camera, const float* jitter, float* rayo, float* rayd, void* stream);
+
+/* ---- camera traces: the trace makes each pixel's ray from the camera itself ----
+ * The counterpart of camera2rays followed by trace_rays (integration_utils/gaussian_renderer/
+ * ever.py:105-121, 189-205) without the (R,6) ray arrays: the rays are those of
+ * ever_camera_rays (same arithmetic, bit for bit). Threads take "slots", 32 per 8x4 pixel
+ * tile, so that a warp traces one tile. Tiles are grouped in 64x64-pixel supertiles
+ * (8 x 16 tiles), supertiles row-major, tiles inside a supertile in Morton order: slot s
+ * lies in supertile u = s / 4096 at (u % ceil(width/64), u / ceil(width/64)), in its tile
+ * w = (s / 32) % 128 at (tx, ty) = bits (0,2,4) and (1,3,5,6) of w, and is pixel
+ * (col, row) = (64 ux + 8 tx + s % 8, 64 uy + 4 ty + (s % 32) / 8), or padding (no pixel)
+ * where that lies outside the image. Per-pixel outputs are indexed by pixel (row-major,
+ * R = width*height); event-log columns are slots (row length ever_camera_slots). */
+
+/* Slot count ceil(width/64) * ceil(height/64) * 4096, or -1 (see ever_last_error). */
+int64_t ever_camera_slots(const EverCamera* camera);
+
+/* slot_pixel (slots): the pixel of each slot, -1 for padding. */
+int ever_camera_slot_pixels(const EverCamera* camera, int32_t* slot_pixel, void* stream);
+
+/* Forward trace of the camera's rays; as ever_trace_forward otherwise (tune->traversal is
+ * ignored: warps always trace their tile as one packet). */
+int ever_trace_forward_camera(const EverScene* scene, const EverCamera* camera, const float* jitter,
+                              const EverTraceArgs* args, const EverTune* tune, const EverForwardOut* out,
+                              void* stream);
+
+/* Backward of ever_trace_forward_camera; as ever_trace_backward otherwise. slot_order
+ * (nullable): launch position -> slot, from ever_camera_backward_slot_order. out->drayo and
+ * out->drayd may both be NULL (camera rays need no gradient); else (R,3) by pixel. */
+int ever_trace_backward_camera(const EverScene* scene, const EverCamera* camera, const float* jitter,
+                               const EverTraceArgs* args, const float* grad_out, const float* states,
+                               const int32_t* iters, const int32_t* event_log, int32_t log_cap, const float* wct,
+                               int32_t num_wct, const float* mean, const float* scale, const float* quat,
+                               void* workspace, size_t workspace_bytes, const int32_t* slot_order,
+                               const EverTune* tune, const EverBackwardOut* out, void* stream);
+
+/* ever_backward_slot_order for a camera trace (iters by pixel; padding slots last).
+ * Workspace: ever_ray_order_workspace_bytes(ever_camera_slots(camera)). */
+int ever_camera_backward_slot_order(const EverCamera* camera, const int32_t* iters, int32_t shift, void* workspace,
+                                    size_t workspace_bytes, int32_t* slot_order, void* stream);
+
+/* ever_event_log_to_reference for a camera trace: tri_collection (max_iters, R) by pixel. */
+int ever_camera_event_log_to_reference(const EverScene* scene, const EverCamera* camera, const int32_t* event_log,
+                                       int32_t log_cap, const int32_t* iters, int32_t* tri_collection,
+                                       int32_t max_iters, void* stream);
 
 #ifdef __cplusplus
 }
