@@ -305,23 +305,25 @@ __global__ void k_gather(const uint32_t* __restrict__ sorted_vals, int64_t N, in
 }
 
 // Feature rows into Morton order, one thread per padded float (coalesced on both sides).
+// Feature rows to Morton order, padded to feat_stride(K): one row per threadIdx.y, one
+// float4 column per threadIdx.x (blockDim.x = feat_stride(K) / 4), so no index division per
+// element. vec: the source rows are whole, 16-byte aligned float4s (3K % 4 == 0, aligned base).
 __global__ void k_gather_features(const int32_t* __restrict__ order, int64_t N, int K, const float* __restrict__ feat,
-                                  float* __restrict__ feat_out) {
-  const int fst = feat_stride(K);
-  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t >= N * fst) return;
-  const int64_t j = t / fst;
-  const int k = int(t - j * fst);
-  feat_out[t] = k < 3 * K ? feat[int64_t(order[j]) * 3 * K + k] : 0.f;
-}
-
-__global__ void k_set_features(const int32_t* __restrict__ order, int64_t N, int K, const float* __restrict__ feat,
-                               float* __restrict__ feat_out) {
-  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  const int64_t per = int64_t(K) * 3;
-  if (t >= N * per) return;
-  const int64_t j = t / per, k = t - j * per;
-  feat_out[j * feat_stride(K) + k] = feat[int64_t(order[j]) * per + k];
+                                  float* __restrict__ feat_out, bool vec) {
+  const int64_t j = int64_t(blockIdx.x) * blockDim.y + threadIdx.y;
+  if (j >= N) return;
+  const int c = threadIdx.x, per = 3 * K;
+  const float* src = feat + int64_t(__ldg(order + j)) * per;
+  float4 v;
+  if (vec) {
+    v = __ldg(reinterpret_cast<const float4*>(src) + c);
+  } else {
+    float t[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) t[q] = 4 * c + q < per ? __ldg(src + 4 * c + q) : 0.f;
+    v = make_float4(t[0], t[1], t[2], t[3]);
+  }
+  reinterpret_cast<float4*>(feat_out + j * feat_stride(K))[c] = v;
 }
 
 // Karras 2012: delta(i, j) = common prefix length of keys i, j (index bits break ties).
@@ -417,6 +419,13 @@ __global__ void k_single_leaf(Node* nodes, const float4* aabb) {
 
 inline int64_t div_up(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+void launch_gather_features(const int32_t* order, int64_t N, int K, const float* feat, float* feat_out,
+                            cudaStream_t st) {
+  const int cols = feat_stride(K) / 4, rows = std::max(1, 256 / cols);
+  const bool vec = (3 * K) % 4 == 0 && reinterpret_cast<uintptr_t>(feat) % 16 == 0;
+  k_gather_features<<<unsigned(div_up(N, rows)), dim3(cols, rows), 0, st>>>(order, N, K, feat, feat_out, vec);
+}
+
 }  // namespace
 
 int sort_blocks(int64_t N) { return int(div_up(std::max<int64_t>(N, 1), kSortTile)); }
@@ -500,7 +509,7 @@ cudaError_t scene_build(const float* mean, const float* scale, const float* quat
   sort_pairs(ka, va, kb, vb, hist, N, 30, st);
   k_gather<<<unsigned(gb), tb, 0, st>>>(va, N, K, mean, scale, quat, density, aabb_a, aabb_b,
                                         reinterpret_cast<Record*>(sc->records), sc->features, sc->order);
-  k_gather_features<<<unsigned(div_up(N * feat_stride(K), tb)), tb, 0, st>>>(sc->order, N, K, feat, sc->features);
+  launch_gather_features(sc->order, N, K, feat, sc->features, st);
   if (N == 1) {
     k_single_leaf<<<1, 1, 0, st>>>(nodes, aabb_b);
     return cudaGetLastError();
@@ -534,7 +543,7 @@ cudaError_t scene_refit(const float* mean, const float* scale, const float* quat
                                         aabb_a, aabb_b, reinterpret_cast<Record*>(sc->records), sc->features,
                                         sc->order);
   if (feat)
-    k_gather_features<<<unsigned(div_up(N * feat_stride(K), tb)), tb, 0, st>>>(sc->order, N, K, feat, sc->features);
+    launch_gather_features(sc->order, N, K, feat, sc->features, st);
   if (N == 1) {
     k_single_leaf<<<1, 1, 0, st>>>(nodes, aabb_b);
     return cudaGetLastError();
@@ -548,8 +557,7 @@ cudaError_t scene_refit(const float* mean, const float* scale, const float* quat
 cudaError_t scene_set_features(EverScene* sc, const float* feat, cudaStream_t st) {
   const int64_t total = sc->num_prims * int64_t(sc->sh_coeffs) * 3;
   if (total == 0) return cudaSuccess;
-  k_set_features<<<unsigned(div_up(total, 256)), 256, 0, st>>>(sc->order, sc->num_prims, sc->sh_coeffs, feat,
-                                                               sc->features);
+  launch_gather_features(sc->order, sc->num_prims, sc->sh_coeffs, feat, sc->features, st);
   return cudaGetLastError();
 }
 

@@ -745,15 +745,25 @@ __global__ void k_finalize(const FinalizeParams P) {
 }
 
 // tri[i * R + ray] from log[i * R + slot], ray = ray_order[slot] (or slot).
-// Feature gradients back to original order and shape (N,K,3), clipped at 1e3; one
-// thread per output float.
+// Feature gradients back to original order and shape (N,K,3), clipped at 1e3: one row per
+// threadIdx.y, one float4 column per threadIdx.x (blockDim.x = feat_stride(K) / 4). vec: the
+// output rows are whole, 16-byte aligned float4s (3K % 4 == 0, aligned base).
 __global__ void k_finalize_features(const int32_t* __restrict__ order, int64_t N, int K,
-                                    const float* __restrict__ acc_feat, float* __restrict__ dfeat) {
-  const int64_t per = int64_t(K) * 3;
-  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t >= N * per) return;
-  const int64_t j = t / per, k = t - j * per;
-  dfeat[int64_t(order[j]) * per + k] = clip_grad(acc_feat[j * feat_stride(K) + k], 1e3f);
+                                    const float* __restrict__ acc_feat, float* __restrict__ dfeat, bool vec) {
+  const int64_t j = int64_t(blockIdx.x) * blockDim.y + threadIdx.y;
+  if (j >= N) return;
+  const int c = threadIdx.x, per = 3 * K;
+  const float4 a = reinterpret_cast<const float4*>(acc_feat + j * feat_stride(K))[c];
+  const float4 g = make_float4(clip_grad(a.x, 1e3f), clip_grad(a.y, 1e3f), clip_grad(a.z, 1e3f), clip_grad(a.w, 1e3f));
+  float* dst = dfeat + int64_t(__ldg(order + j)) * per;
+  if (vec) {
+    reinterpret_cast<float4*>(dst)[c] = g;
+  } else {
+    const float t[4] = {g.x, g.y, g.z, g.w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (4 * c + q < per) dst[4 * c + q] = t[q];
+  }
 }
 
 __global__ void k_log_to_reference(const int32_t* __restrict__ order, const int32_t* __restrict__ log, int log_cap,
@@ -884,8 +894,10 @@ cudaError_t launch_camera_log_to_reference(const CameraParams& cam, const int32_
 cudaError_t launch_finalize(const FinalizeParams& P, cudaStream_t st) {
   if (P.N == 0) return cudaSuccess;
   k_finalize<<<unsigned((P.N + 255) / 256), 256, 0, st>>>(P);
-  const int64_t total = P.N * int64_t(P.K) * 3;
-  k_finalize_features<<<unsigned((total + 255) / 256), 256, 0, st>>>(P.order, P.N, P.K, P.acc_feat, P.out.dfeatures);
+  const int cols = feat_stride(P.K) / 4, rows = 256 / cols > 0 ? 256 / cols : 1;
+  const bool vec = (3 * P.K) % 4 == 0 && reinterpret_cast<uintptr_t>(P.out.dfeatures) % 16 == 0;
+  k_finalize_features<<<unsigned((P.N + rows - 1) / rows), dim3(cols, rows), 0, st>>>(P.order, P.N, P.K, P.acc_feat,
+                                                                                     P.out.dfeatures, vec);
   return cudaGetLastError();
 }
 
