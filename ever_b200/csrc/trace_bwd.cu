@@ -403,8 +403,7 @@ __device__ __forceinline__ float3 load3(const float* v, int64_t r) {
 // Reverse replay of ray r = (ro, rd) (event-log column `slot`) against scene S. Ray
 // gradients are written to P.drayo / P.drayd row r unless those are null.
 template <int DEG>
-__device__ void backward_ray(const BScene& S, const BRayCtx& P, int64_t r, int64_t slot, float3 ro, float3 rd,
-                             int* st_node, int stride) {
+__device__ void backward_ray(const BScene& S, const BRayCtx& P, int64_t r, int64_t slot, float3 ro, float3 rd) {
   const int n = P.iters[r];
   if (n >= P.max_iters - 1 || n <= 0) {  // backwards_kernel.slang:304
     if (P.drayo) {
@@ -558,6 +557,9 @@ __device__ void backward_ray(const BScene& S, const BRayCtx& P, int64_t r, int64
 
   // initial density: backwards_initial_drgb_kernel, backwards_kernel.slang:374-428
   if (G.drgb.x != 0.f || G.drgb.y != 0.f || G.drgb.z != 0.f || G.drgb.w != 0.f) {
+    // point-query stack in local memory: only rays that start inside ellipsoids touch it,
+    // and the kernels keep all of the SM's on-chip memory as L1 for the scattered loads
+    int st_node[kStackDepth];
     int sp = 0, node = 0;
     for (;;) {
       const float4* np = reinterpret_cast<const float4*>(nodes + node);
@@ -582,7 +584,7 @@ __device__ void backward_ray(const BScene& S, const BRayCtx& P, int64_t r, int64
       }
       const bool i0 = h0 && ch[0] >= 0, i1 = h1 && ch[1] >= 0;
       if (i0 && i1) {
-        if (sp < kStackDepth) st_node[(sp++) * stride] = ch[1];
+        if (sp < kStackDepth) st_node[sp++] = ch[1];
         node = ch[0];
       } else if (i0) {
         node = ch[0];
@@ -590,7 +592,7 @@ __device__ void backward_ray(const BScene& S, const BRayCtx& P, int64_t r, int64
         node = ch[1];
       } else {
         if (sp == 0) break;
-        node = st_node[(--sp) * stride];
+        node = st_node[--sp];
       }
     }
   }
@@ -618,7 +620,6 @@ __device__ void backward_ray(const BScene& S, const BRayCtx& P, int64_t r, int64
 // few spilled bytes, which 16 resident warps hide better than 40 more registers would.
 template <int DEG>
 __global__ void __launch_bounds__(256, 2) k_trace_bwd(const BwdParams P) {
-  extern __shared__ int smem[];
   const int tid = threadIdx.x;
   const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;
   if (gi >= P.R) return;
@@ -628,7 +629,7 @@ __global__ void __launch_bounds__(256, 2) k_trace_bwd(const BwdParams P) {
                  P.acc_geo, P.acc_feat};
   const BRayCtx C{P.rayo, P.rayd, P.tmin, P.max_iters, P.grad_out, P.states, P.iters, P.event_log, P.R,
                   P.drayo, P.drayd, P.wct, P.num_wct, P.dmeans2d};
-  backward_ray<DEG>(S, C, r, slot, load3(P.rayo, r), load3(P.rayd, r), smem + tid, blockDim.x);
+  backward_ray<DEG>(S, C, r, slot, load3(P.rayo, r), load3(P.rayd, r));
 }
 
 // Backward of a camera trace: threads take slots (through the slot order, if any), make
@@ -636,7 +637,6 @@ __global__ void __launch_bounds__(256, 2) k_trace_bwd(const BwdParams P) {
 template <int DEG>
 __global__ void __launch_bounds__(256, 2)
     k_trace_bwd_camera(const BwdParams P, const CameraParams cam, const float* __restrict__ jitter) {
-  extern __shared__ int smem[];
   const int tid = threadIdx.x;
   const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;
   if (gi >= P.R) return;
@@ -649,7 +649,7 @@ __global__ void __launch_bounds__(256, 2)
                   P.drayo, P.drayd, P.wct, P.num_wct, P.dmeans2d};
   float3 ro, rd;
   camera_ray(cam, jitter, p, ro, rd);
-  backward_ray<DEG>(S, C, p, slot, ro, rd, smem + tid, blockDim.x);
+  backward_ray<DEG>(S, C, p, slot, ro, rd);
 }
 
 // Persistent batched backward: warps take 32-slot packets from a device counter. With a
@@ -658,7 +658,6 @@ __global__ void __launch_bounds__(256, 2)
 // own view by binary search over the views' slot ranges.
 template <int DEG>
 __global__ void __launch_bounds__(256, 2) k_trace_bwd_batched(const BatchBwdParams P) {
-  extern __shared__ int smem[];
   const int tid = threadIdx.x, lane = tid & 31;
   const BRayCtx C{P.rayo, P.rayd, P.tmin, P.max_iters, P.grad_out, P.states, P.iters, P.event_log, P.num_slots,
                   P.drayo, P.drayd, nullptr, 0, nullptr};
@@ -681,7 +680,7 @@ __global__ void __launch_bounds__(256, 2) k_trace_bwd_batched(const BatchBwdPara
     const BScene S{reinterpret_cast<const Node*>(bs_.nodes), reinterpret_cast<const Record*>(bs_.records),
                    bs_.features, bs_.K, bs_.acc_geo, bs_.acc_feat};
     const int32_t r = P.slot_ray[slot];
-    if (r >= 0) backward_ray<DEG>(S, C, r, slot, load3(P.rayo, r), load3(P.rayd, r), smem + tid, blockDim.x);
+    if (r >= 0) backward_ray<DEG>(S, C, r, slot, load3(P.rayo, r), load3(P.rayd, r));
     __syncwarp();
   }
 }
@@ -744,7 +743,6 @@ __global__ void k_finalize(const FinalizeParams P) {
   }
 }
 
-// tri[i * R + ray] from log[i * R + slot], ray = ray_order[slot] (or slot).
 // Feature gradients back to original order and shape (N,K,3), clipped at 1e3: one row per
 // threadIdx.y, one float4 column per threadIdx.x (blockDim.x = feat_stride(K) / 4). vec: the
 // output rows are whole, 16-byte aligned float4s (3K % 4 == 0, aligned base).
@@ -766,6 +764,7 @@ __global__ void k_finalize_features(const int32_t* __restrict__ order, int64_t N
   }
 }
 
+// tri[i * R + ray] from log[i * R + slot], ray = ray_order[slot] (or slot).
 __global__ void k_log_to_reference(const int32_t* __restrict__ order, const int32_t* __restrict__ log, int log_cap,
                                    const int32_t* __restrict__ iters, int64_t R, const int32_t* __restrict__ ray_order,
                                    int32_t* __restrict__ tri, int max_iters) {
@@ -783,12 +782,7 @@ __global__ void k_log_to_reference(const int32_t* __restrict__ order, const int3
 
 template <int DEG>
 cudaError_t launch_b(const BwdParams& P, int block, cudaStream_t st) {
-  const size_t smem = size_t(kStackDepth) * block * sizeof(int);
-  auto kern = k_trace_bwd<DEG>;
-  cudaError_t e = cudaSuccess;
-  if (smem > 48 * 1024) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  if (e != cudaSuccess) return e;
-  kern<<<unsigned((P.R + block - 1) / block), block, smem, st>>>(P);
+  k_trace_bwd<DEG><<<unsigned((P.R + block - 1) / block), block, 0, st>>>(P);
   return cudaGetLastError();
 }
 
@@ -796,12 +790,7 @@ cudaError_t launch_b(const BwdParams& P, int block, cudaStream_t st) {
 
 template <int DEG>
 cudaError_t launch_bc(const BwdParams& P, const CameraParams& cam, const float* jitter, int block, cudaStream_t st) {
-  const size_t smem = size_t(kStackDepth) * block * sizeof(int);
-  auto kern = k_trace_bwd_camera<DEG>;
-  cudaError_t e = cudaSuccess;
-  if (smem > 48 * 1024) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  if (e != cudaSuccess) return e;
-  kern<<<unsigned((P.R + block - 1) / block), block, smem, st>>>(P, cam, jitter);
+  k_trace_bwd_camera<DEG><<<unsigned((P.R + block - 1) / block), block, 0, st>>>(P, cam, jitter);
   return cudaGetLastError();
 }
 
@@ -829,14 +818,9 @@ __global__ void k_camera_log_to_reference(const CameraParams cam, int64_t num_sl
 
 template <int DEG>
 cudaError_t launch_bb(const BatchBwdParams& P, int block, cudaStream_t st) {
-  const size_t smem = size_t(kStackDepth) * block * sizeof(int);
-  auto kern = k_trace_bwd_batched<DEG>;
-  cudaError_t e = cudaSuccess;
-  if (smem > 48 * 1024) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  cudaError_t e = cudaMemsetAsync(P.work_counter, 0, sizeof(unsigned int), st);
   if (e != cudaSuccess) return e;
-  e = cudaMemsetAsync(P.work_counter, 0, sizeof(unsigned int), st);
-  if (e != cudaSuccess) return e;
-  kern<<<P.grid, block, smem, st>>>(P);
+  k_trace_bwd_batched<DEG><<<P.grid, block, 0, st>>>(P);
   return cudaGetLastError();
 }
 
