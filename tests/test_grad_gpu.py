@@ -77,6 +77,32 @@ def test_gradients_match_fp64_oracle(deg, seed):
         assert _rel_err(g[k], _clip(k, ref[k])) < GRAD_TOL, (k, _rel_err(g[k], _clip(k, ref[k])))
 
 
+def test_gradients_nested_ellipsoids():
+    # Up to 8 ellipsoids open at once along a ray: the backward holds at most two open
+    # ellipsoids' colour gradients per ray, so this exercises its evictions and the rows
+    # left open at the end of the replay.
+    rng = np.random.default_rng(7)
+    n = 8
+    r = np.linspace(0.1, 0.8, n)
+    mean = rng.normal(0.0, 0.02, (n, 3)).astype(np.float32)
+    scale = (r[:, None] * rng.uniform(0.8, 1.2, (n, 3))).astype(np.float32)
+    quat = rng.normal(size=(n, 4)).astype(np.float32)
+    quat /= np.linalg.norm(quat, axis=1, keepdims=True)
+    density = rng.uniform(0.1, 0.4, (n, 1)).astype(np.float32)
+    features = rng.normal(0.0, 0.3, (n, 16, 3)).astype(np.float32)
+    sc = S.SceneArrays(mean, scale, quat, density, features)
+    ro, rd = S.look_at_rays(S.Camera(np.array([0.3, -0.2, 3.0]), 16, 16, 12.0))
+    dout = rng.normal(size=(ro.shape[0], 5))
+    g, _ = _gpu_grads(sc, ro, rd, dout)
+    ref = _oracle_grads(sc, ro, rd, dout)
+    rep = _oracle_grads(sc, ro, rd, dout, mode="f32_replay")
+    tr = O.trace(O.Scene(mean, scale, quat, density.reshape(-1), features), ro, rd, 0.0, 1000.0, 500)
+    assert tr.iters.max() >= 12  # rays cross most of the shells: many ellipsoids open at once
+    for k in ref:
+        assert _rel_err(g[k], _clip(k, rep[k])) < REPLAY_TOL, (k, _rel_err(g[k], _clip(k, rep[k])))
+        assert _rel_err(g[k], _clip(k, ref[k])) < GRAD_TOL, (k, _rel_err(g[k], _clip(k, ref[k])))
+
+
 def test_gradients_rays_inside_and_tmin():
     sc = S.uniform_scene(1200, 3, seed=5)
     sc.scale *= 2.5
