@@ -277,6 +277,47 @@ def _timed(fn, dev):
     return a.elapsed_time(b)
 
 
+def leg_camera(dev, args, reps=5):
+    """Camera traces: trace_camera (rays made in the kernels, warps on 8x4 pixel tiles, no
+    ray arrays and no ray sort) against camera_rays + trace_rays (ray arrays, coherent sort)
+    on the bench scene and view, forward + backward through torch.autograd with the BVH
+    build, as the headline step. Median of `reps` steps each; images compared bit for bit."""
+    import torch
+    from ever_b200 import camera as CAM
+    from ever_b200 import synthetic as S
+    from ever_b200.fast_ellipsoid_splinetracer import trace_rays
+    sc = S.clustered_scene(args.prims, 3, seed=2)
+    w, h, f, c2w = S.pinhole(S.Camera(S.sphere_point(4.0, 2), args.width, args.height, 50.0))
+    cam = CAM.Camera(w, h, f, f, c2w)
+    prm = [torch.tensor(np.ascontiguousarray(a), device=dev, requires_grad=True)
+           for a in (sc.mean, sc.scale, sc.quat, sc.density, sc.features)]
+    del sc
+    gout = torch.randn((w * h, 5), device=dev, generator=torch.Generator(device=dev).manual_seed(0))
+    outs = {}
+
+    def via_rays():
+        ro, rd = CAM.camera_rays(w, h, f, f, c2w, device=dev)
+        out = trace_rays(*prm, ro, rd, 0.0, 1000.0)
+        torch.autograd.grad((out * gout).sum(), prm)
+        outs["rays"] = out.detach()
+
+    def via_camera():
+        out = CAM.trace_camera(*prm, cam, 0.0, 1000.0)
+        torch.autograd.grad((out * gout).sum(), prm)
+        outs["camera"] = out.detach()
+
+    ms = {}
+    for name, fn in (("rays", via_rays), ("camera", via_camera)):
+        fn()
+        ms[name] = float(np.median([_timed(fn, dev) for _ in range(reps)]))
+    R = w * h
+    return {"workload": f"{args.prims} clustered ellipsoids SH3, one {w}x{h} pinhole view, forward + backward "
+                        f"with the BVH build per step",
+            "ms": ms, "mrays": {k: R / (v * 1e-3) / 1e6 for k, v in ms.items()},
+            "speedup_camera_vs_rays": ms["rays"] / ms["camera"],
+            "images_bit_identical": bool(torch.equal(outs["rays"], outs["camera"]))}
+
+
 def leg_batched(dev, reps=3):
     """Several scenes of uneven size and views of mixed resolution: per-view launches
     against one persistent forward + backward over all views (CUDA graph), with the
@@ -685,6 +726,7 @@ def main():
                                 "sample": f"{n} seeded rays of the view, forward + FP64 backward, {dt:.1f} s"}
         line["cpu_baselines_small"] = small_cpu_baselines(threads)
     if rank == 0 and world == 1 and not args.no_batched:
+        line["camera"] = leg_camera(dev, args)
         line["batched"] = leg_batched(dev)
     if rank == 0 and world == 1 and not args.no_sched:
         line["sched"] = leg_sched(dev, args.sched_views)

@@ -102,6 +102,20 @@ def look_at_rays(cam: Camera):
     return np.ascontiguousarray(o, np.float32), np.ascontiguousarray(d, np.float32)
 
 
+def pinhole(cam: Camera):
+    """The look-at camera as (width, height, f, c2w 3x4) of a pinhole with the principal
+    point at the image centre (x right, y down, z forward): the rays of look_at_rays."""
+    eye = np.asarray(cam.eye, np.float64)
+    fwd = -eye / np.linalg.norm(eye)
+    up = np.array([0.0, 0.0, 1.0]) if abs(fwd[2]) < 0.99 else np.array([0.0, 1.0, 0.0])
+    right = np.cross(fwd, up)
+    right /= np.linalg.norm(right)
+    upv = np.cross(right, fwd)
+    f = 0.5 * cam.height / np.tan(0.5 * np.deg2rad(cam.fov_y_deg))
+    c2w = np.stack([right, -upv, fwd, eye], axis=1)
+    return cam.width, cam.height, f, c2w
+
+
 def look_at_rays_device(cam: Camera, device):
     """look_at_rays computed with torch on `device` (float64, then float32): same rays up to
     the last float32 bit, without the host round trip for large views."""
