@@ -74,6 +74,10 @@ SIGNATURES = {
     "ever_scene_set_features": (ctypes.c_int, [ctypes.POINTER(EverScene), c_p, c_p]),
     "ever_trace_forward": (ctypes.c_int, [ctypes.POINTER(EverScene), c_p, c_p, c_i64, ctypes.POINTER(EverTraceArgs),
                                           c_p, ctypes.POINTER(EverTune), ctypes.POINTER(EverForwardOut), c_p]),
+    "ever_trace_forward_workspace_bytes": (c_sz, [c_i64]),
+    "ever_trace_forward_regrouped": (ctypes.c_int, [ctypes.POINTER(EverScene), c_p, c_p, c_i64,
+                                                    ctypes.POINTER(EverTraceArgs), c_p, ctypes.POINTER(EverTune),
+                                                    ctypes.POINTER(EverForwardOut), c_p, c_sz, c_p]),
     "ever_backward_workspace_bytes": (c_sz, [c_i64, c_i32]),
     "ever_trace_backward": (ctypes.c_int, [ctypes.POINTER(EverScene), c_p, c_p, c_i64, ctypes.POINTER(EverTraceArgs),
                                            c_p, c_p, c_p, c_p, c_i32, c_p, c_i32, c_p, c_p, c_p, c_p, c_sz, c_p,

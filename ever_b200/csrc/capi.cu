@@ -135,6 +135,46 @@ int ever_trace_forward(const EverScene* scene, const float* rayo, const float* r
                      "ever_trace_forward");
 }
 
+size_t ever_trace_forward_workspace_bytes(int64_t num_rays) {
+  if (num_rays < 0 || num_rays >= (int64_t(1) << 31)) return 0;
+  return size_t(ever::regroup_workspace(num_rays));
+}
+
+int ever_trace_forward_regrouped(const EverScene* scene, const float* rayo, const float* rayd, int64_t num_rays,
+                                 const EverTraceArgs* args, const int32_t* ray_order, const EverTune* tune,
+                                 const EverForwardOut* out, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!scene || !args || !out) return fail(EVER_ERR_INVALID, "null scene, args or out");
+  if (num_rays < 0 || num_rays >= (int64_t(1) << 31)) return fail(EVER_ERR_INVALID, "num_rays out of range");
+  if (num_rays > 0 && (!rayo || !rayd || !out->out || !out->iters || !out->states || !out->last_dirac))
+    return fail(EVER_ERR_INVALID, "null rayo, rayd, out, iters, states or last_dirac");
+  if (out->event_log && out->log_cap < 0) return fail(EVER_ERR_INVALID, "negative log_cap");
+  const int64_t need = ever::regroup_workspace(num_rays);
+  if (num_rays > 0 && (!workspace || workspace_bytes < size_t(need)))
+    return fail(EVER_ERR_WORKSPACE, "forward workspace needs %lld bytes, got %zu", (long long)need, workspace_bytes);
+  if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0) return fail(EVER_ERR_INVALID, "workspace not 256-byte aligned");
+  int deg = 0;
+  if (int rc = resolve_degree(scene, args, &deg)) return rc;
+  ever::FwdParams P{};
+  P.nodes = scene->nodes;
+  P.records = scene->records;
+  P.features = scene->features;
+  P.order = scene->order;
+  P.N = scene->num_prims;
+  P.K = scene->sh_coeffs;
+  P.rayo = rayo;
+  P.rayd = rayd;
+  P.R = num_rays;
+  P.tmin = args->tmin;
+  P.tmax = args->tmax;
+  P.max_iters = args->max_iters;
+  P.ray_order = ray_order;
+  P.out = *out;
+  if (num_rays == 0) return EVER_OK;
+  const ever::RegroupScratch W = ever::regroup_scratch(static_cast<char*>(workspace), num_rays);
+  return cuda_status(ever::launch_forward_regrouped(P, W, deg, resolve_tune(tune), static_cast<cudaStream_t>(stream)),
+                     "ever_trace_forward_regrouped");
+}
+
 size_t ever_backward_workspace_bytes(int64_t num_prims, int32_t sh_coeffs) {
   if (num_prims < 0 || sh_coeffs < 1) return 0;
   ever::WsCursor c;

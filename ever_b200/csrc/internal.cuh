@@ -73,6 +73,30 @@ struct FwdParams {
 };
 
 cudaError_t launch_forward(const FwdParams& P, int deg, const EverTune& tune, cudaStream_t st);
+
+// Regrouped forward (warp packets): round 0 for every ray, then the rays still active are
+// packed into full warps for round 1, and again for the remaining rounds. Scratch in the
+// caller's workspace; P.out.states and P.out.last_dirac hold the parked rays' loop state.
+struct RegroupScratch {
+  uint32_t* mask0;    // ceil(R/32): lanes of each pass-0 warp still active
+  uint32_t* mask1;    // ceil(R/32): the same for pass 1
+  uint32_t* offsets;  // ceil(R/32) + 1: exclusive scan of a mask's popcounts
+  int32_t* list1;     // R: slots of pass 1, in slot order
+  int32_t* list2;     // R: slots of pass 2
+  uint32_t* count1;   // 1
+  uint32_t* count2;   // 1
+};
+int64_t regroup_workspace(int64_t R);
+RegroupScratch regroup_scratch(char* ws, int64_t R);
+// dst = the entries of src (identity if null) at the positions whose mask bit is set, in
+// order; *dst_count = their number. n: number of positions (*n_dev if given, else n_max).
+cudaError_t regroup_compact(const uint32_t* mask, const uint32_t* n_dev, int64_t n_max, const int32_t* src,
+                            uint32_t* offsets, int32_t* dst, uint32_t* dst_count, cudaStream_t st);
+cudaError_t launch_forward_regrouped(const FwdParams& P, const RegroupScratch& W, int deg, const EverTune& tune,
+                                     cudaStream_t st);
+template <int KBUF>
+cudaError_t launch_forward_regrouped_k(const FwdParams& P, const RegroupScratch& W, int deg, int block,
+                                       cudaStream_t st);
 // Per k-buffer size launchers (trace_fwd_k8.cu, trace_fwd_k16.cu, trace_fwd_k32.cu).
 template <int KBUF>
 cudaError_t launch_forward_k(const FwdParams& P, int deg, int block, int traversal, cudaStream_t st);

@@ -21,6 +21,8 @@
 // inside the reference round that consumed its entry. The result is the reference's
 // event sequence for any KBUF.
 #pragma once
+#include <climits>
+
 #include "camera.cuh"
 #include "common.cuh"
 #include "internal.cuh"
@@ -438,42 +440,112 @@ __global__ void __launch_bounds__(256) k_trace_fwd_ray(const FwdParams P) {
   write_outputs(C.out, r, s, last_dirac, iters, status);
 }
 
+// The SH basis of the ray's direction into the block's shared array (B[k * bs]).
+template <int DEG>
+__device__ __forceinline__ void store_basis(const Ray& ray, float* B, int bs) {
+  float Bl[16];
+  sh_basis<DEG>(ray.rd, Bl);
+#pragma unroll
+  for (int k = 0; k < (DEG + 1) * (DEG + 1); ++k) B[k * bs] = Bl[k];
+}
+
+// What a ray carries from one gather round to the next. cnt16 is not kept: it always equals
+// iters % kRefRound (both count the consumed events from zero).
+struct RayLoop {
+  State s;
+  float4 last_dirac;
+  int iters;
+  float s16;
+  int cnt16;
+  uint64_t lower;
+  uint32_t status;
+};
+
+// Initial state of a ray: empty, plus the density of the ellipsoids its start lies in.
+template <int DEG>
+__device__ __forceinline__ RayLoop start_ray(const SceneRef& sc, const Ray& ray, bool valid, int* wstack, float* B,
+                                             int bs, int lane) {
+  RayLoop L;
+  L.status = 0;
+  L.s = empty_state();
+  L.last_dirac = make_float4(0.f, 0.f, 0.f, 0.f);
+  L.iters = 0;
+  L.s16 = 0.f;
+  L.cnt16 = 0;
+  L.lower = 0;
+  if (sc.N > 0) {
+    int mem_p[kMaxMembers], mem_j[kMaxMembers];
+    float4 extra = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int n_mem = point_members<DEG, true>(sc.nodes, sc.recs, sc.features, feat_stride(sc.K), B, bs, ray, valid,
+                                               wstack, 1, lane, mem_p, mem_j, extra, L.status);
+    init_density<DEG>(sc, B, bs, n_mem, mem_j, extra, L.status, L.s);
+  }
+  return L;
+}
+
+// Gather + consume rounds of a warp's packet until no lane is active or max_rounds rounds
+// have run. Returns whether this lane's ray needs another round.
+template <int KBUF, int DEG>
+__device__ __forceinline__ bool run_rounds(const SceneRef& sc, const TraceCtx& C, const Ray& ray, const float* B, int bs,
+                                           int64_t slot, int* wstack, int lane, bool act, RayLoop& L, int max_rounds) {
+  const RaySlab sl = make_slab(ray);
+  for (int round = 0; round < max_rounds && __any_sync(kFull, act); ++round) {
+    uint64_t buf[KBUF];
+#pragma unroll
+    for (int i = 0; i < KBUF; ++i) buf[i] = kEmptyKey;
+    gather_packet<KBUF>(sc.nodes, sc.recs, ray, sl, act, L.lower, L.s16, C.tmax, buf, wstack, lane, L.status);
+    if (act)
+      act = !consume<KBUF, DEG>(sc, C, ray, B, bs, slot, buf, L.s, L.last_dirac, L.iters, L.s16, L.cnt16, L.lower,
+                                L.status);
+  }
+  return act;
+}
+
 // One warp traces one packet of up to 32 rays against one scene (lanes with valid=false
 // only take part in the warp-wide votes).
 template <int KBUF, int DEG>
 __device__ __forceinline__ void trace_packet(const SceneRef& sc, const TraceCtx& C, const Ray& ray, int64_t r,
                                              bool valid, int64_t slot, int* wstack, float* B, int bs, int lane) {
-  const RaySlab sl = make_slab(ray);
-  {
-    float Bl[16];
-    sh_basis<DEG>(ray.rd, Bl);
-#pragma unroll
-    for (int k = 0; k < (DEG + 1) * (DEG + 1); ++k) B[k * bs] = Bl[k];
-  }
-  uint32_t status = 0;
-  State s = empty_state();
-  float4 last_dirac = make_float4(0.f, 0.f, 0.f, 0.f);
-  int iters = 0;
-  if (sc.N > 0) {
-    int mem_p[kMaxMembers], mem_j[kMaxMembers];
-    float4 extra = make_float4(0.f, 0.f, 0.f, 0.f);
-    const int n_mem = point_members<DEG, true>(sc.nodes, sc.recs, sc.features, feat_stride(sc.K), B, bs, ray, valid,
-                                               wstack, 1, lane, mem_p, mem_j, extra, status);
-    init_density<DEG>(sc, B, bs, n_mem, mem_j, extra, status, s);
-    float s16 = 0.f;
-    int cnt16 = 0;
-    uint64_t lower = 0;
-    bool act = valid && C.max_iters > 0;
-    while (__any_sync(kFull, act)) {
-      uint64_t buf[KBUF];
-#pragma unroll
-      for (int i = 0; i < KBUF; ++i) buf[i] = kEmptyKey;
-      gather_packet<KBUF>(sc.nodes, sc.recs, ray, sl, act, lower, s16, C.tmax, buf, wstack, lane, status);
-      if (act) act = !consume<KBUF, DEG>(sc, C, ray, B, bs, slot, buf, s, last_dirac, iters, s16, cnt16, lower, status);
-    }
-  }
-  if (valid) write_outputs(C.out, r, s, last_dirac, iters, status);
+  store_basis<DEG>(ray, B, bs);
+  RayLoop L = start_ray<DEG>(sc, ray, valid, wstack, B, bs, lane);
+  run_rounds<KBUF, DEG>(sc, C, ray, B, bs, slot, wstack, lane, valid && C.max_iters > 0 && sc.N > 0, L, INT_MAX);
+  if (valid) write_outputs(C.out, r, L.s, L.last_dirac, L.iters, L.status);
   __syncwarp();
+}
+
+// A ray that needs more rounds parks its loop state in its own output rows: `states` in
+// the final layout, with s16 and the 64-bit key bound of the next round in the three
+// padding words, `last_dirac` and `iters`. Its status flags are raised now.
+__device__ __forceinline__ void park_ray(const EverForwardOut& out, int64_t r, const RayLoop& L) {
+  float4* st = reinterpret_cast<float4*>(out.states + 16 * r);
+  st[0] = make_float4(L.s.dist_x, L.s.dist_y, L.s.cum_x, L.s.cum_y);
+  st[1] = make_float4(L.s16, __uint_as_float(uint32_t(L.lower)), __uint_as_float(uint32_t(L.lower >> 32)), L.s.t);
+  st[2] = L.s.drgb;
+  st[3] = make_float4(L.s.logT, L.s.C.x, L.s.C.y, L.s.C.z);
+  reinterpret_cast<float4*>(out.last_dirac)[r] = L.last_dirac;
+  out.iters[r] = L.iters;
+  if (L.status && out.status) atomicOr(out.status, int(L.status));
+}
+
+__device__ __forceinline__ RayLoop resume_ray(const EverForwardOut& out, int64_t r) {
+  const float4* st = reinterpret_cast<const float4*>(out.states + 16 * r);
+  const float4 a = st[0], b = st[1], c = st[2], d = st[3];
+  RayLoop L;
+  L.s.dist_x = a.x;
+  L.s.dist_y = a.y;
+  L.s.cum_x = a.z;
+  L.s.cum_y = a.w;
+  L.s.t = b.w;
+  L.s.drgb = c;
+  L.s.logT = d.x;
+  L.s.C = make_float3(d.y, d.z, d.w);
+  L.s16 = b.x;
+  L.lower = uint64_t(__float_as_uint(b.y)) | (uint64_t(__float_as_uint(b.z)) << 32);
+  L.last_dirac = reinterpret_cast<const float4*>(out.last_dirac)[r];
+  L.iters = out.iters[r];
+  L.cnt16 = L.iters % kRefRound;
+  L.status = 0;
+  return L;
 }
 
 // Resident blocks per SM that the register budget of the packet kernels targets: 20
@@ -496,6 +568,51 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value) k_trace_fwd
   const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out};
   const Ray ray = load_ray(P.rayo, P.rayd, r, P.tmin);
   trace_packet<KBUF, DEG>(scene_of(P), C, ray, r, valid, gi, wstack, B, blockDim.x, lane);
+}
+
+// Regrouped forward, one pass. PASS 0 takes every slot in order and runs the first gather
+// round; PASS 1 runs one more round and PASS 2 every remaining round, each for the slots in
+// `list` (count entries): the rays that the previous pass left active, packed into full
+// warps in slot order. Passes 0 and 1 park the rays that still need rounds and write one
+// lane mask per warp (mask[position / 32]); the other rays write their outputs.
+template <int KBUF, int DEG, int BLOCK, int PASS>
+__global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value)
+    k_trace_fwd_pass(const FwdParams P, const int32_t* __restrict__ list, const uint32_t* __restrict__ count,
+                     uint32_t* __restrict__ mask) {
+  extern __shared__ int smem[];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int* wstack = smem + warp * kStackDepth;
+  float* B = reinterpret_cast<float*>(smem + (blockDim.x / 32) * kStackDepth) + tid;
+  const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;  // slot (PASS 0) or list position
+  const int64_t n = PASS == 0 ? P.R : int64_t(*count);
+  if ((gi & ~int64_t(31)) >= n) return;  // the whole warp lies beyond the list
+  const bool valid = gi < n;
+  const int64_t slot = valid ? (PASS == 0 ? gi : int64_t(list[gi])) : 0;
+  const int64_t r = valid ? (P.ray_order ? int64_t(P.ray_order[slot]) : slot) : 0;
+  const SceneRef sc = scene_of(P);
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out};
+  const Ray ray = load_ray(P.rayo, P.rayd, r, P.tmin);
+  store_basis<DEG>(ray, B, blockDim.x);
+  RayLoop L;
+  bool act;
+  if (PASS == 0) {
+    L = start_ray<DEG>(sc, ray, valid, wstack, B, blockDim.x, lane);
+    act = valid && C.max_iters > 0 && sc.N > 0;
+  } else {
+    if (valid) L = resume_ray(P.out, r);
+    act = valid;
+  }
+  act = run_rounds<KBUF, DEG>(sc, C, ray, B, blockDim.x, slot, wstack, lane, act, L, PASS == 2 ? INT_MAX : 1);
+  if (PASS < 2) {
+    const unsigned m = __ballot_sync(kFull, act);
+    if (lane == 0) mask[gi >> 5] = m;
+  }
+  if (valid) {
+    if (PASS < 2 && act)
+      park_ray(P.out, r, L);
+    else
+      write_outputs(C.out, r, L.s, L.last_dirac, L.iters, L.status);
+  }
 }
 
 // Camera trace: rays are made from the camera in the kernel (no ray arrays). The launch
@@ -573,6 +690,39 @@ cudaError_t launch_k(const FwdParams& P, int deg, int block, int traversal, cuda
     case 1: return launch_t<KBUF, 1>(P, block, traversal, st);
     case 2: return launch_t<KBUF, 2>(P, block, traversal, st);
     default: return launch_t<KBUF, 3>(P, block, traversal, st);
+  }
+}
+
+template <int KBUF, int DEG, int BLOCK>
+cudaError_t launch_regrouped_b(const FwdParams& P, const RegroupScratch& W, cudaStream_t st) {
+  const unsigned grid = unsigned((P.R + BLOCK - 1) / BLOCK);
+  const size_t smem = size_t(kStackDepth) * (BLOCK / 32) * sizeof(int) + size_t(16) * BLOCK * sizeof(float);
+  k_trace_fwd_pass<KBUF, DEG, BLOCK, 0><<<grid, BLOCK, smem, st>>>(P, nullptr, nullptr, W.mask0);
+  cudaError_t e = regroup_compact(W.mask0, nullptr, P.R, nullptr, W.offsets, W.list1, W.count1, st);
+  if (e != cudaSuccess) return e;
+  k_trace_fwd_pass<KBUF, DEG, BLOCK, 1><<<grid, BLOCK, smem, st>>>(P, W.list1, W.count1, W.mask1);
+  e = regroup_compact(W.mask1, W.count1, P.R, W.list1, W.offsets, W.list2, W.count2, st);
+  if (e != cudaSuccess) return e;
+  k_trace_fwd_pass<KBUF, DEG, BLOCK, 2><<<grid, BLOCK, smem, st>>>(P, W.list2, W.count2, nullptr);
+  return cudaGetLastError();
+}
+
+template <int KBUF, int DEG>
+cudaError_t launch_regrouped_t(const FwdParams& P, const RegroupScratch& W, int block, cudaStream_t st) {
+  switch (block) {
+    case 64: return launch_regrouped_b<KBUF, DEG, 64>(P, W, st);
+    case 128: return launch_regrouped_b<KBUF, DEG, 128>(P, W, st);
+    default: return launch_regrouped_b<KBUF, DEG, 256>(P, W, st);
+  }
+}
+
+template <int KBUF>
+cudaError_t launch_regrouped_k(const FwdParams& P, const RegroupScratch& W, int deg, int block, cudaStream_t st) {
+  switch (deg) {
+    case 0: return launch_regrouped_t<KBUF, 0>(P, W, block, st);
+    case 1: return launch_regrouped_t<KBUF, 1>(P, W, block, st);
+    case 2: return launch_regrouped_t<KBUF, 2>(P, W, block, st);
+    default: return launch_regrouped_t<KBUF, 3>(P, W, block, st);
   }
 }
 

@@ -15,6 +15,12 @@ cudaError_t launch_forward_camera_k<8>(const FwdParams& P, const CameraParams& c
 }
 
 template <>
+cudaError_t launch_forward_regrouped_k<8>(const FwdParams& P, const RegroupScratch& W, int deg, int block,
+                                            cudaStream_t st) {
+  return launch_regrouped_k<8>(P, W, deg, block, st);
+}
+
+template <>
 cudaError_t launch_forward_batched_k<8>(const BatchFwdParams& P, int deg, int block, cudaStream_t st) {
   return launch_batched_k<8>(P, deg, block, st);
 }

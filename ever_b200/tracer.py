@@ -133,7 +133,12 @@ def trace_args(tmin, tmax, max_iters, sh_degree):
 
 def forward(scene: Scene, rayo, rayd, tmin=0.0, tmax=1000.0, max_iters=500, sh_degree=None, log_events=True,
             touch_count=False, ray_stats=False, ray_order=None, tune: Tune | None = None,
-            buffers: ForwardResult | None = None) -> ForwardResult:
+            buffers: ForwardResult | None = None, regrouped: bool = True,
+            workspace: torch.Tensor | None = None) -> ForwardResult:
+    """regrouped: with warp packets (tune.traversal 0) and k-buffers of up to 16 events,
+    re-pack the rays that need more gather rounds into full warps between passes
+    (ever_trace_forward_regrouped; same results, faster). workspace: optional uint8 scratch
+    of ever_trace_forward_workspace_bytes(R)."""
     device = scene.device
     _check_tensor("ray_origins", rayo, device, 3)
     _check_tensor("ray_directions", rayd, device, 3)
@@ -163,10 +168,23 @@ def forward(scene: Scene, rayo, rayd, tmin=0.0, tmax=1000.0, max_iters=500, sh_d
     o.ray_stats = N.ptr(buffers.ray_stats)
     o.status = N.ptr(buffers.status)
     args = trace_args(tmin, tmax, max_iters, sh_degree)
+    tune = tune or Tune()
+    lib = N.load()
     with torch.cuda.device(device):
-        N.check(N.load().ever_trace_forward(ctypes.byref(scene.c), N.ptr(rayo), N.ptr(rayd), R, ctypes.byref(args),
-                                            N.ptr(ray_order), ctypes.byref((tune or Tune()).c()), ctypes.byref(o),
-                                            _stream(device)))
+        # the packed passes pay for buffers of up to 16 events; with 32, most rays finish in
+        # the first round and the extra passes only add their overhead
+        if regrouped and tune.traversal == 0 and tune.kbuf <= 16 and R < (1 << 31):
+            need = int(lib.ever_trace_forward_workspace_bytes(R))
+            if workspace is None or workspace.numel() < need:
+                workspace = torch.empty(max(need, 256), dtype=torch.uint8, device=device)
+            N.check(lib.ever_trace_forward_regrouped(ctypes.byref(scene.c), N.ptr(rayo), N.ptr(rayd), R,
+                                                     ctypes.byref(args), N.ptr(ray_order), ctypes.byref(tune.c()),
+                                                     ctypes.byref(o), N.ptr(workspace), int(workspace.numel()),
+                                                     _stream(device)))
+        else:
+            N.check(lib.ever_trace_forward(ctypes.byref(scene.c), N.ptr(rayo), N.ptr(rayd), R, ctypes.byref(args),
+                                           N.ptr(ray_order), ctypes.byref(tune.c()), ctypes.byref(o),
+                                           _stream(device)))
     return buffers
 
 

@@ -133,6 +133,20 @@ int ever_trace_forward(const EverScene* scene, const float* rayo, const float* r
                        const EverTraceArgs* args, const int32_t* ray_order, const EverTune* tune,
                        const EverForwardOut* out, void* stream);
 
+/* Bytes of workspace ever_trace_forward_regrouped() needs for R rays (0 if R is out of
+ * range). */
+size_t ever_trace_forward_workspace_bytes(int64_t num_rays);
+
+/* ever_trace_forward, same arguments and the same results bit for bit, for warp-packet
+ * traversal (tune->traversal is ignored), and faster: after each of the first two gather
+ * rounds the rays that need more rounds are packed into full warps in launch order, so
+ * warps stop running with most of their lanes idle. Rays between passes keep their loop
+ * state in out->states and out->last_dirac, which are therefore required. R < 2^31.
+ * No counterpart in the reference (OptiX runs one thread per ray to the end). */
+int ever_trace_forward_regrouped(const EverScene* scene, const float* rayo, const float* rayd, int64_t num_rays,
+                                 const EverTraceArgs* args, const int32_t* ray_order, const EverTune* tune,
+                                 const EverForwardOut* out, void* workspace, size_t workspace_bytes, void* stream);
+
 /* Bytes of gradient-accumulation workspace ever_trace_backward() needs. */
 size_t ever_backward_workspace_bytes(int64_t num_prims, int32_t sh_coeffs);
 
