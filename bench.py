@@ -690,9 +690,10 @@ def main():
     achieved = b_dom / (ph[dom] * 1e-3) / 1e9
     # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one single-pass
     # ncu capture of `bench.py --once` on this default workload (1M ellipsoids, 1920x1080)
-    measured_traffic = {"fwd": 213_023_232 + 371_919_104, "bwd": 2_754_422_528 + 399_600_896}
+    # (forward: the three passes of the regrouped forward together)
+    measured_traffic = {"fwd": 507_734_016 + 439_507_712, "bwd": 2_763_808_768 + 398_342_912}
     default_workload = args.prims == 1_000_000 and args.width == 1920 and args.height == 1080
-    roofline = {"bound": "hbm", "kernel": "k_trace_bwd" if dom == "bwd" else "k_trace_fwd",
+    roofline = {"bound": "hbm", "kernel": "k_trace_bwd" if dom == "bwd" else "k_trace_fwd_pass (3 passes)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind, "traffic": measured_traffic[dom] if default_workload else None,
                 "algorithmic_bytes": b_dom}

@@ -85,6 +85,7 @@ struct RegroupScratch {
   int32_t* list2;     // R: slots of pass 2
   uint32_t* count1;   // 1
   uint32_t* count2;   // 1
+  int64_t split_min;  // a pass with fewer rays runs every remaining round (set by the launcher)
 };
 int64_t regroup_workspace(int64_t R);
 RegroupScratch regroup_scratch(char* ws, int64_t R);

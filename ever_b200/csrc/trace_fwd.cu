@@ -107,6 +107,7 @@ RegroupScratch regroup_scratch(char* ws, int64_t R) {
   W.list2 = reinterpret_cast<int32_t*>(ws + c.take(R * 4));
   W.count1 = reinterpret_cast<uint32_t*>(ws + c.take(4));
   W.count2 = reinterpret_cast<uint32_t*>(ws + c.take(4));
+  W.split_min = 0;
   return W;
 }
 
@@ -121,10 +122,21 @@ cudaError_t launch_forward_regrouped(const FwdParams& P, const RegroupScratch& W
                                      cudaStream_t st) {
   if (P.R == 0) return cudaSuccess;
   const int block = tune.block > 0 ? tune.block : 128;
+  // splitting pays only while the next pass still fills the GPU several times over: four
+  // times the resident lanes of the packet kernels (20 warps per SM)
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  RegroupScratch V = W;
+  V.split_min = tune.regroup_min > 0 ? int64_t(tune.regroup_min) : int64_t(4) * sms * 20 * 32;
+  if (P.R < V.split_min) {  // one pass would run every round: the single packet kernel does the same
+    EverTune t = tune;
+    t.traversal = 0;
+    return launch_forward(P, deg, t, st);
+  }
   switch (tune.kbuf) {
-    case 8: return launch_forward_regrouped_k<8>(P, W, deg, block, st);
-    case 32: return launch_forward_regrouped_k<32>(P, W, deg, block, st);
-    default: return launch_forward_regrouped_k<16>(P, W, deg, block, st);
+    case 8: return launch_forward_regrouped_k<8>(P, V, deg, block, st);
+    case 32: return launch_forward_regrouped_k<32>(P, V, deg, block, st);
+    default: return launch_forward_regrouped_k<16>(P, V, deg, block, st);
   }
 }
 

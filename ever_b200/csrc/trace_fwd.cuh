@@ -573,12 +573,14 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value) k_trace_fwd
 // Regrouped forward, one pass. PASS 0 takes every slot in order and runs the first gather
 // round; PASS 1 runs one more round and PASS 2 every remaining round, each for the slots in
 // `list` (count entries): the rays that the previous pass left active, packed into full
-// warps in slot order. Passes 0 and 1 park the rays that still need rounds and write one
+// warps in slot order. A pass 0 or 1 with fewer than `split_min` rays runs every remaining
+// round instead (a later pass would hold too few rays to fill the GPU, and its latency-bound
+// tail would run alone). Passes 0 and 1 park the rays that still need rounds and write one
 // lane mask per warp (mask[position / 32]); the other rays write their outputs.
 template <int KBUF, int DEG, int BLOCK, int PASS>
 __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value)
     k_trace_fwd_pass(const FwdParams P, const int32_t* __restrict__ list, const uint32_t* __restrict__ count,
-                     uint32_t* __restrict__ mask) {
+                     uint32_t* __restrict__ mask, int64_t split_min) {
   extern __shared__ int smem[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   int* wstack = smem + warp * kStackDepth;
@@ -602,7 +604,8 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value)
     if (valid) L = resume_ray(P.out, r);
     act = valid;
   }
-  act = run_rounds<KBUF, DEG>(sc, C, ray, B, blockDim.x, slot, wstack, lane, act, L, PASS == 2 ? INT_MAX : 1);
+  const bool last = PASS == 2 || n < split_min;
+  act = run_rounds<KBUF, DEG>(sc, C, ray, B, blockDim.x, slot, wstack, lane, act, L, last ? INT_MAX : 1);
   if (PASS < 2) {
     const unsigned m = __ballot_sync(kFull, act);
     if (lane == 0) mask[gi >> 5] = m;
@@ -697,13 +700,13 @@ template <int KBUF, int DEG, int BLOCK>
 cudaError_t launch_regrouped_b(const FwdParams& P, const RegroupScratch& W, cudaStream_t st) {
   const unsigned grid = unsigned((P.R + BLOCK - 1) / BLOCK);
   const size_t smem = size_t(kStackDepth) * (BLOCK / 32) * sizeof(int) + size_t(16) * BLOCK * sizeof(float);
-  k_trace_fwd_pass<KBUF, DEG, BLOCK, 0><<<grid, BLOCK, smem, st>>>(P, nullptr, nullptr, W.mask0);
+  k_trace_fwd_pass<KBUF, DEG, BLOCK, 0><<<grid, BLOCK, smem, st>>>(P, nullptr, nullptr, W.mask0, W.split_min);
   cudaError_t e = regroup_compact(W.mask0, nullptr, P.R, nullptr, W.offsets, W.list1, W.count1, st);
   if (e != cudaSuccess) return e;
-  k_trace_fwd_pass<KBUF, DEG, BLOCK, 1><<<grid, BLOCK, smem, st>>>(P, W.list1, W.count1, W.mask1);
+  k_trace_fwd_pass<KBUF, DEG, BLOCK, 1><<<grid, BLOCK, smem, st>>>(P, W.list1, W.count1, W.mask1, W.split_min);
   e = regroup_compact(W.mask1, W.count1, P.R, W.list1, W.offsets, W.list2, W.count2, st);
   if (e != cudaSuccess) return e;
-  k_trace_fwd_pass<KBUF, DEG, BLOCK, 2><<<grid, BLOCK, smem, st>>>(P, W.list2, W.count2, nullptr);
+  k_trace_fwd_pass<KBUF, DEG, BLOCK, 2><<<grid, BLOCK, smem, st>>>(P, W.list2, W.count2, nullptr, 0);
   return cudaGetLastError();
 }
 

@@ -37,10 +37,11 @@ class Tune:
     kbuf: int = 16
     block: int = 128
     traversal: int = 0  # 0: warp packets, 1: one walk per ray
+    regroup_min: int = 0  # regrouped forward: rays below which a pass runs every remaining round (0: auto)
 
     def c(self):
         t = N.EverTune()
-        t.kbuf, t.block, t.traversal = self.kbuf, self.block, self.traversal
+        t.kbuf, t.block, t.traversal, t.regroup_min = self.kbuf, self.block, self.traversal, self.regroup_min
         return t
 
 

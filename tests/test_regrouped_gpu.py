@@ -25,6 +25,9 @@ def _scene(dev, sc):
 
 
 def _both(scene, ro, rd, max_iters=500, tmin=0.0, tmax=1000.0, order=None, tune=None):
+    # regroup_min=1: every pass hands its remaining rays on, whatever their number (the
+    # default keeps small launches in one pass)
+    tune = tune or T.Tune(regroup_min=1)
     kw = dict(touch_count=True, ray_stats=True, ray_order=order, tune=tune)
     a = T.forward(scene, ro, rd, tmin, tmax, max_iters, regrouped=False, **kw)
     b = T.forward(scene, ro, rd, tmin, tmax, max_iters, regrouped=True, **kw)
@@ -52,7 +55,7 @@ def test_regrouped_equals_single_kernel(kbuf, block, ordered):
     scene = _scene(dev, _thin_scene(20_000, 2, 51))
     ro, rd = S.look_at_rays_device(S.Camera(S.sphere_point(3.0, 51), 45, 37, 40.0), dev)  # 1665 rays
     order = T.ray_order(ro, rd) if ordered else None
-    a = _both(scene, ro, rd, order=order, tune=T.Tune(kbuf, block, 0))
+    a = _both(scene, ro, rd, order=order, tune=T.Tune(kbuf, block, 0, regroup_min=1))
     assert int(a.iters.max()) > 2 * kbuf  # rays reach the last pass
     assert int((a.iters < kbuf).sum()) > 0  # and others finish in the first
 
@@ -103,3 +106,13 @@ def test_regrouped_many_rays():
     ro, rd = S.look_at_rays_device(S.Camera(S.sphere_point(3.0, 55), 640, 480, 45.0), dev)
     a = _both(scene, ro, rd, order=T.ray_order(ro, rd))
     assert int((a.iters > 32).sum()) > 10_000
+
+
+@pytest.mark.parametrize("regroup_min", [0, 1000, 100_000])
+def test_regrouped_split_threshold(regroup_min):
+    # 0 (four times the resident lanes: here one pass), and thresholds that split only the
+    # first pass or none: the results never change
+    dev = _dev()
+    scene = _scene(dev, _thin_scene(20_000, 2, 56))
+    ro, rd = S.look_at_rays_device(S.Camera(S.sphere_point(3.0, 56), 45, 37, 40.0), dev)
+    _both(scene, ro, rd, order=T.ray_order(ro, rd), tune=T.Tune(16, 128, 0, regroup_min=regroup_min))
