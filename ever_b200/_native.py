@@ -123,6 +123,9 @@ SIGNATURES = {
     "ever_trace_forward_camera": (ctypes.c_int, [ctypes.POINTER(EverScene), ctypes.POINTER(EverCamera), c_p,
                                                  ctypes.POINTER(EverTraceArgs), ctypes.POINTER(EverTune),
                                                  ctypes.POINTER(EverForwardOut), c_p]),
+    "ever_trace_forward_camera_regrouped": (ctypes.c_int, [ctypes.POINTER(EverScene), ctypes.POINTER(EverCamera),
+                                                           c_p, ctypes.POINTER(EverTraceArgs), ctypes.POINTER(EverTune),
+                                                           ctypes.POINTER(EverForwardOut), c_p, c_sz, c_p]),
     "ever_trace_backward_camera": (ctypes.c_int, [ctypes.POINTER(EverScene), ctypes.POINTER(EverCamera), c_p,
                                                   ctypes.POINTER(EverTraceArgs), c_p, c_p, c_p, c_p, c_i32, c_p,
                                                   c_i32, c_p, c_p, c_p, c_p, c_sz, c_p, ctypes.POINTER(EverTune),

@@ -124,8 +124,11 @@ def slot_pixels(camera: Camera, device=None) -> torch.Tensor:
 
 
 def forward(scene: T.Scene, camera: Camera, jitter=None, tmin=0.0, tmax=1000.0, max_iters=500, sh_degree=None,
-            log_events=True, touch_count=False, ray_stats=False, tune: T.Tune | None = None) -> T.ForwardResult:
-    """Forward trace of the camera's pixels; results by pixel, event-log columns by slot."""
+            log_events=True, touch_count=False, ray_stats=False, tune: T.Tune | None = None,
+            regrouped: bool = True) -> T.ForwardResult:
+    """Forward trace of the camera's pixels; results by pixel, event-log columns by slot.
+    regrouped: with k-buffers of up to 16 events, pack the pixels still active after the
+    first gather rounds into full warps (ever_trace_forward_camera_regrouped; same results)."""
     device = scene.device
     R, S = camera.num_pixels, camera_slots(camera)
     jitter = _jitter(jitter, R, device)
@@ -146,10 +149,20 @@ def forward(scene: T.Scene, camera: Camera, jitter=None, tmin=0.0, tmax=1000.0, 
     o.ray_stats = N.ptr(res.ray_stats)
     o.status = N.ptr(res.status)
     args = T.trace_args(tmin, tmax, max_iters, sh_degree)
+    tune = tune or T.Tune()
+    lib = N.load()
     with torch.cuda.device(device):
-        N.check(N.load().ever_trace_forward_camera(ctypes.byref(scene.c), ctypes.byref(camera.c()), N.ptr(jitter),
-                                                   ctypes.byref(args), ctypes.byref((tune or T.Tune()).c()),
-                                                   ctypes.byref(o), _stream(device)))
+        if regrouped and tune.kbuf <= 16:
+            ws = torch.empty(max(int(lib.ever_trace_forward_workspace_bytes(S)), 256), dtype=torch.uint8,
+                             device=device)
+            N.check(lib.ever_trace_forward_camera_regrouped(ctypes.byref(scene.c), ctypes.byref(camera.c()),
+                                                            N.ptr(jitter), ctypes.byref(args), ctypes.byref(tune.c()),
+                                                            ctypes.byref(o), N.ptr(ws), int(ws.numel()),
+                                                            _stream(device)))
+        else:
+            N.check(lib.ever_trace_forward_camera(ctypes.byref(scene.c), ctypes.byref(camera.c()), N.ptr(jitter),
+                                                  ctypes.byref(args), ctypes.byref(tune.c()), ctypes.byref(o),
+                                                  _stream(device)))
     return res
 
 

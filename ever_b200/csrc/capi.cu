@@ -171,7 +171,8 @@ int ever_trace_forward_regrouped(const EverScene* scene, const float* rayo, cons
   P.out = *out;
   if (num_rays == 0) return EVER_OK;
   const ever::RegroupScratch W = ever::regroup_scratch(static_cast<char*>(workspace), num_rays);
-  return cuda_status(ever::launch_forward_regrouped(P, W, deg, resolve_tune(tune), static_cast<cudaStream_t>(stream)),
+  return cuda_status(ever::launch_forward_regrouped(P, W, nullptr, nullptr, deg, resolve_tune(tune),
+                                                    static_cast<cudaStream_t>(stream)),
                      "ever_trace_forward_regrouped");
 }
 
@@ -396,6 +397,42 @@ int ever_trace_forward_camera(const EverScene* scene, const EverCamera* camera, 
   return cuda_status(
       ever::launch_forward_camera(P, C, jitter, deg, resolve_tune(tune), static_cast<cudaStream_t>(stream)),
       "ever_trace_forward_camera");
+}
+
+int ever_trace_forward_camera_regrouped(const EverScene* scene, const EverCamera* camera, const float* jitter,
+                                        const EverTraceArgs* args, const EverTune* tune, const EverForwardOut* out,
+                                        void* workspace, size_t workspace_bytes, void* stream) {
+  if (!scene || !args || !out) return fail(EVER_ERR_INVALID, "null scene, args or out");
+  ever::CameraParams C{};
+  if (const char* msg = ever::camera_params(camera, &C))
+    return fail(EVER_ERR_INVALID, "ever_trace_forward_camera_regrouped: %s", msg);
+  const int64_t R = int64_t(C.width) * C.height, S = ever::camera_slots(C);
+  if (R > 0 && (!out->out || !out->iters || !out->states || !out->last_dirac))
+    return fail(EVER_ERR_INVALID, "null out, iters, states or last_dirac");
+  if (out->event_log && out->log_cap < 0) return fail(EVER_ERR_INVALID, "negative log_cap");
+  const int64_t need = ever::regroup_workspace(S);
+  if (R > 0 && (!workspace || workspace_bytes < size_t(need)))
+    return fail(EVER_ERR_WORKSPACE, "forward workspace needs %lld bytes, got %zu", (long long)need, workspace_bytes);
+  if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0) return fail(EVER_ERR_INVALID, "workspace not 256-byte aligned");
+  int deg = 0;
+  if (int rc = resolve_degree(scene, args, &deg)) return rc;
+  ever::FwdParams P{};
+  P.nodes = scene->nodes;
+  P.records = scene->records;
+  P.features = scene->features;
+  P.order = scene->order;
+  P.N = scene->num_prims;
+  P.K = scene->sh_coeffs;
+  P.R = R;
+  P.tmin = args->tmin;
+  P.tmax = args->tmax;
+  P.max_iters = args->max_iters;
+  P.out = *out;
+  if (R == 0) return EVER_OK;
+  const ever::RegroupScratch W = ever::regroup_scratch(static_cast<char*>(workspace), S);
+  return cuda_status(ever::launch_forward_regrouped(P, W, &C, jitter, deg, resolve_tune(tune),
+                                                    static_cast<cudaStream_t>(stream)),
+                     "ever_trace_forward_camera_regrouped");
 }
 
 int ever_trace_backward_camera(const EverScene* scene, const EverCamera* camera, const float* jitter,

@@ -93,11 +93,14 @@ RegroupScratch regroup_scratch(char* ws, int64_t R);
 // order; *dst_count = their number. n: number of positions (*n_dev if given, else n_max).
 cudaError_t regroup_compact(const uint32_t* mask, const uint32_t* n_dev, int64_t n_max, const int32_t* src,
                             uint32_t* offsets, int32_t* dst, uint32_t* dst_count, cudaStream_t st);
-cudaError_t launch_forward_regrouped(const FwdParams& P, const RegroupScratch& W, int deg, const EverTune& tune,
-                                     cudaStream_t st);
+struct CameraParams;
+// cam: null for the ray arrays of P, else the camera whose slots are traced (rays made in
+// the kernels, P.R = its pixel count) with the per-pixel jitter (nullable).
+cudaError_t launch_forward_regrouped(const FwdParams& P, const RegroupScratch& W, const CameraParams* cam,
+                                     const float* jitter, int deg, const EverTune& tune, cudaStream_t st);
 template <int KBUF>
-cudaError_t launch_forward_regrouped_k(const FwdParams& P, const RegroupScratch& W, int deg, int block,
-                                       cudaStream_t st);
+cudaError_t launch_forward_regrouped_k(const FwdParams& P, const RegroupScratch& W, const CameraParams* cam,
+                                       const float* jitter, int deg, int block, cudaStream_t st);
 // Per k-buffer size launchers (trace_fwd_k8.cu, trace_fwd_k16.cu, trace_fwd_k32.cu).
 template <int KBUF>
 cudaError_t launch_forward_k(const FwdParams& P, int deg, int block, int traversal, cudaStream_t st);

@@ -1,5 +1,6 @@
 // Forward trace dispatch: k-buffer size -> the instantiations in trace_fwd_k{8,16,32}.cu
 // (kernels in trace_fwd.cuh).
+#include "camera.cuh"
 #include "common.cuh"
 #include "internal.cuh"
 
@@ -118,8 +119,8 @@ cudaError_t regroup_compact(const uint32_t* mask, const uint32_t* n_dev, int64_t
   return cudaGetLastError();
 }
 
-cudaError_t launch_forward_regrouped(const FwdParams& P, const RegroupScratch& W, int deg, const EverTune& tune,
-                                     cudaStream_t st) {
+cudaError_t launch_forward_regrouped(const FwdParams& P, const RegroupScratch& W, const CameraParams* cam,
+                                     const float* jitter, int deg, const EverTune& tune, cudaStream_t st) {
   if (P.R == 0) return cudaSuccess;
   const int block = tune.block > 0 ? tune.block : 128;
   // splitting pays only while the next pass still fills the GPU several times over: four
@@ -128,15 +129,16 @@ cudaError_t launch_forward_regrouped(const FwdParams& P, const RegroupScratch& W
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   RegroupScratch V = W;
   V.split_min = tune.regroup_min > 0 ? int64_t(tune.regroup_min) : int64_t(4) * sms * 20 * 32;
-  if (P.R < V.split_min) {  // one pass would run every round: the single packet kernel does the same
+  const int64_t n = cam ? camera_slots(*cam) : P.R;
+  if (n < V.split_min) {  // one pass would run every round: the single packet kernel does the same
     EverTune t = tune;
     t.traversal = 0;
-    return launch_forward(P, deg, t, st);
+    return cam ? launch_forward_camera(P, *cam, jitter, deg, t, st) : launch_forward(P, deg, t, st);
   }
   switch (tune.kbuf) {
-    case 8: return launch_forward_regrouped_k<8>(P, V, deg, block, st);
-    case 32: return launch_forward_regrouped_k<32>(P, V, deg, block, st);
-    default: return launch_forward_regrouped_k<16>(P, V, deg, block, st);
+    case 8: return launch_forward_regrouped_k<8>(P, V, cam, jitter, deg, block, st);
+    case 32: return launch_forward_regrouped_k<32>(P, V, cam, jitter, deg, block, st);
+    default: return launch_forward_regrouped_k<16>(P, V, cam, jitter, deg, block, st);
   }
 }
 

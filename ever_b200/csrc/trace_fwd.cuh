@@ -577,23 +577,47 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value) k_trace_fwd
 // round instead (a later pass would hold too few rays to fill the GPU, and its latency-bound
 // tail would run alone). Passes 0 and 1 park the rays that still need rounds and write one
 // lane mask per warp (mask[position / 32]); the other rays write their outputs.
-template <int KBUF, int DEG, int BLOCK, int PASS>
+// Camera passes (CAM): slots are the camera's (camera.cuh); a slot's pixel ray is made in
+// the kernel, padding slots take part only in the warp votes, and the event log has one
+// column per slot.
+struct PassCamera {
+  CameraParams cam;
+  const float* jitter;
+  int64_t num_slots;
+};
+
+template <int KBUF, int DEG, int BLOCK, int PASS, bool CAM>
 __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value)
     k_trace_fwd_pass(const FwdParams P, const int32_t* __restrict__ list, const uint32_t* __restrict__ count,
-                     uint32_t* __restrict__ mask, int64_t split_min) {
+                     uint32_t* __restrict__ mask, int64_t split_min, const PassCamera Q) {
   extern __shared__ int smem[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   int* wstack = smem + warp * kStackDepth;
   float* B = reinterpret_cast<float*>(smem + (blockDim.x / 32) * kStackDepth) + tid;
   const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;  // slot (PASS 0) or list position
-  const int64_t n = PASS == 0 ? P.R : int64_t(*count);
+  const int64_t slots = CAM ? Q.num_slots : P.R;
+  const int64_t n = PASS == 0 ? slots : int64_t(*count);
   if ((gi & ~int64_t(31)) >= n) return;  // the whole warp lies beyond the list
-  const bool valid = gi < n;
-  const int64_t slot = valid ? (PASS == 0 ? gi : int64_t(list[gi])) : 0;
-  const int64_t r = valid ? (P.ray_order ? int64_t(P.ray_order[slot]) : slot) : 0;
+  const int64_t slot = gi < n ? (PASS == 0 ? gi : int64_t(list[gi])) : 0;
+  int64_t r = 0;
+  bool valid = gi < n;
+  if (CAM) {
+    r = valid ? camera_slot_pixel(Q.cam, slot) : -1;
+    valid = r >= 0;
+  } else if (valid) {
+    r = P.ray_order ? int64_t(P.ray_order[slot]) : slot;
+  }
+  if (!valid) r = 0;
   const SceneRef sc = scene_of(P);
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out};
-  const Ray ray = load_ray(P.rayo, P.rayd, r, P.tmin);
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, slots, P.out};
+  Ray ray;
+  if (CAM) {
+    float3 ro, rd;
+    camera_ray(Q.cam, Q.jitter, r, ro, rd);
+    ray = make_ray(ro, rd, P.tmin);
+  } else {
+    ray = load_ray(P.rayo, P.rayd, r, P.tmin);
+  }
   store_basis<DEG>(ray, B, blockDim.x);
   RayLoop L;
   bool act;
@@ -696,37 +720,52 @@ cudaError_t launch_k(const FwdParams& P, int deg, int block, int traversal, cuda
   }
 }
 
-template <int KBUF, int DEG, int BLOCK>
-cudaError_t launch_regrouped_b(const FwdParams& P, const RegroupScratch& W, cudaStream_t st) {
-  const unsigned grid = unsigned((P.R + BLOCK - 1) / BLOCK);
+template <int KBUF, int DEG, int BLOCK, bool CAM>
+cudaError_t launch_regrouped_b(const FwdParams& P, const RegroupScratch& W, const PassCamera& Q, cudaStream_t st) {
+  const int64_t n = CAM ? Q.num_slots : P.R;
+  const unsigned grid = unsigned((n + BLOCK - 1) / BLOCK);
   const size_t smem = size_t(kStackDepth) * (BLOCK / 32) * sizeof(int) + size_t(16) * BLOCK * sizeof(float);
-  k_trace_fwd_pass<KBUF, DEG, BLOCK, 0><<<grid, BLOCK, smem, st>>>(P, nullptr, nullptr, W.mask0, W.split_min);
-  cudaError_t e = regroup_compact(W.mask0, nullptr, P.R, nullptr, W.offsets, W.list1, W.count1, st);
+  k_trace_fwd_pass<KBUF, DEG, BLOCK, 0, CAM><<<grid, BLOCK, smem, st>>>(P, nullptr, nullptr, W.mask0, W.split_min, Q);
+  cudaError_t e = regroup_compact(W.mask0, nullptr, n, nullptr, W.offsets, W.list1, W.count1, st);
   if (e != cudaSuccess) return e;
-  k_trace_fwd_pass<KBUF, DEG, BLOCK, 1><<<grid, BLOCK, smem, st>>>(P, W.list1, W.count1, W.mask1, W.split_min);
-  e = regroup_compact(W.mask1, W.count1, P.R, W.list1, W.offsets, W.list2, W.count2, st);
+  k_trace_fwd_pass<KBUF, DEG, BLOCK, 1, CAM><<<grid, BLOCK, smem, st>>>(P, W.list1, W.count1, W.mask1, W.split_min, Q);
+  e = regroup_compact(W.mask1, W.count1, n, W.list1, W.offsets, W.list2, W.count2, st);
   if (e != cudaSuccess) return e;
-  k_trace_fwd_pass<KBUF, DEG, BLOCK, 2><<<grid, BLOCK, smem, st>>>(P, W.list2, W.count2, nullptr, 0);
+  k_trace_fwd_pass<KBUF, DEG, BLOCK, 2, CAM><<<grid, BLOCK, smem, st>>>(P, W.list2, W.count2, nullptr, 0, Q);
   return cudaGetLastError();
 }
 
-template <int KBUF, int DEG>
-cudaError_t launch_regrouped_t(const FwdParams& P, const RegroupScratch& W, int block, cudaStream_t st) {
+template <int KBUF, int DEG, bool CAM>
+cudaError_t launch_regrouped_t(const FwdParams& P, const RegroupScratch& W, const PassCamera& Q, int block,
+                               cudaStream_t st) {
   switch (block) {
-    case 64: return launch_regrouped_b<KBUF, DEG, 64>(P, W, st);
-    case 128: return launch_regrouped_b<KBUF, DEG, 128>(P, W, st);
-    default: return launch_regrouped_b<KBUF, DEG, 256>(P, W, st);
+    case 64: return launch_regrouped_b<KBUF, DEG, 64, CAM>(P, W, Q, st);
+    case 128: return launch_regrouped_b<KBUF, DEG, 128, CAM>(P, W, Q, st);
+    default: return launch_regrouped_b<KBUF, DEG, 256, CAM>(P, W, Q, st);
   }
 }
 
-template <int KBUF>
-cudaError_t launch_regrouped_k(const FwdParams& P, const RegroupScratch& W, int deg, int block, cudaStream_t st) {
+template <int KBUF, bool CAM>
+cudaError_t launch_regrouped_c(const FwdParams& P, const RegroupScratch& W, const PassCamera& Q, int deg, int block,
+                               cudaStream_t st) {
   switch (deg) {
-    case 0: return launch_regrouped_t<KBUF, 0>(P, W, block, st);
-    case 1: return launch_regrouped_t<KBUF, 1>(P, W, block, st);
-    case 2: return launch_regrouped_t<KBUF, 2>(P, W, block, st);
-    default: return launch_regrouped_t<KBUF, 3>(P, W, block, st);
+    case 0: return launch_regrouped_t<KBUF, 0, CAM>(P, W, Q, block, st);
+    case 1: return launch_regrouped_t<KBUF, 1, CAM>(P, W, Q, block, st);
+    case 2: return launch_regrouped_t<KBUF, 2, CAM>(P, W, Q, block, st);
+    default: return launch_regrouped_t<KBUF, 3, CAM>(P, W, Q, block, st);
   }
+}
+
+// cam: null for ray arrays, else the camera (its slots) and the per-pixel jitter
+template <int KBUF>
+cudaError_t launch_regrouped_k(const FwdParams& P, const RegroupScratch& W, const CameraParams* cam,
+                               const float* jitter, int deg, int block, cudaStream_t st) {
+  PassCamera Q{};
+  if (!cam) return launch_regrouped_c<KBUF, false>(P, W, Q, deg, block, st);
+  Q.cam = *cam;
+  Q.jitter = jitter;
+  Q.num_slots = camera_slots(*cam);
+  return launch_regrouped_c<KBUF, true>(P, W, Q, deg, block, st);
 }
 
 template <int KBUF, int DEG>

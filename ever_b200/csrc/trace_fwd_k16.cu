@@ -15,9 +15,9 @@ cudaError_t launch_forward_camera_k<16>(const FwdParams& P, const CameraParams& 
 }
 
 template <>
-cudaError_t launch_forward_regrouped_k<16>(const FwdParams& P, const RegroupScratch& W, int deg, int block,
-                                            cudaStream_t st) {
-  return launch_regrouped_k<16>(P, W, deg, block, st);
+cudaError_t launch_forward_regrouped_k<16>(const FwdParams& P, const RegroupScratch& W, const CameraParams* cam,
+                                            const float* jitter, int deg, int block, cudaStream_t st) {
+  return launch_regrouped_k<16>(P, W, cam, jitter, deg, block, st);
 }
 
 template <>

@@ -15,9 +15,9 @@ cudaError_t launch_forward_camera_k<8>(const FwdParams& P, const CameraParams& c
 }
 
 template <>
-cudaError_t launch_forward_regrouped_k<8>(const FwdParams& P, const RegroupScratch& W, int deg, int block,
-                                            cudaStream_t st) {
-  return launch_regrouped_k<8>(P, W, deg, block, st);
+cudaError_t launch_forward_regrouped_k<8>(const FwdParams& P, const RegroupScratch& W, const CameraParams* cam,
+                                            const float* jitter, int deg, int block, cudaStream_t st) {
+  return launch_regrouped_k<8>(P, W, cam, jitter, deg, block, st);
 }
 
 template <>

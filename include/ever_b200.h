@@ -406,6 +406,14 @@ int ever_trace_forward_camera(const EverScene* scene, const EverCamera* camera, 
                               const EverTraceArgs* args, const EverTune* tune, const EverForwardOut* out,
                               void* stream);
 
+/* ever_trace_forward_camera with the passes of ever_trace_forward_regrouped (the same
+ * results bit for bit): out->states and out->last_dirac are required, and the workspace
+ * holds ever_trace_forward_workspace_bytes(ever_camera_slots(camera)) bytes. No counterpart
+ * in the reference. */
+int ever_trace_forward_camera_regrouped(const EverScene* scene, const EverCamera* camera, const float* jitter,
+                                        const EverTraceArgs* args, const EverTune* tune, const EverForwardOut* out,
+                                        void* workspace, size_t workspace_bytes, void* stream);
+
 /* Backward of ever_trace_forward_camera; as ever_trace_backward otherwise. slot_order
  * (nullable): launch position -> slot, from ever_camera_backward_slot_order. out->drayo and
  * out->drayd may both be NULL (camera rays need no gradient); else (R,3) by pixel. */

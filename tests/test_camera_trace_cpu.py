@@ -79,3 +79,27 @@ def test_camera_trace_validation():
     assert lib.ever_camera_backward_slot_order(ctypes.byref(cam), fake, 17, fake, ws_need, fake, None) == 1
     assert lib.ever_camera_slot_pixels(ctypes.byref(cam), None, None) == 1
     assert lib.ever_camera_event_log_to_reference(None, ctypes.byref(cam), None, 0, None, None, 5, None) == 1
+
+
+def test_camera_regrouped_validation():
+    lib = N.load()
+    sc = N.EverScene()
+    sc.num_prims, sc.sh_coeffs = 0, 1
+    args = N.EverTraceArgs()
+    args.max_iters, args.sh_degree = 10, -1
+    out = N.EverForwardOut()
+    fake = ctypes.c_void_p(256)
+    out.out, out.iters = fake, fake
+    cam = _cam(4, 4)
+    rc = lib.ever_trace_forward_camera_regrouped(ctypes.byref(sc), ctypes.byref(cam), None, ctypes.byref(args), None,
+                                                 ctypes.byref(out), None, 0, None)
+    assert rc == 1 and b"states" in lib.ever_last_error()
+    out.states, out.last_dirac = fake, fake
+    need = lib.ever_trace_forward_workspace_bytes(lib.ever_camera_slots(ctypes.byref(cam)))
+    rc = lib.ever_trace_forward_camera_regrouped(ctypes.byref(sc), ctypes.byref(cam), None, ctypes.byref(args), None,
+                                                 ctypes.byref(out), fake, need - 1, None)
+    assert rc == 3
+    rc = lib.ever_trace_forward_regrouped(ctypes.byref(sc), fake, fake, 100, ctypes.byref(args), None, None,
+                                          ctypes.byref(out), fake, 0, None)
+    assert rc == 3 and b"workspace" in lib.ever_last_error()
+    assert lib.ever_trace_forward_workspace_bytes(-1) == 0 and lib.ever_trace_forward_workspace_bytes(1 << 31) == 0

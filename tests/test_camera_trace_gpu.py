@@ -205,3 +205,24 @@ def test_camera_trace_truncation_and_empty_cases():
     assert torch.equal(f0.out, torch.zeros_like(f0.out))
     g0 = CAM.backward(s0, cam, f0, torch.ones_like(f0.out), want_ray_grads=True)
     assert torch.equal(g0.rayd, torch.zeros_like(g0.rayd))
+
+
+@pytest.mark.parametrize("kbuf,block", [(16, 128), (8, 64), (16, 256)])
+@pytest.mark.parametrize("jitter", [False, True])
+def test_camera_regrouped_equals_single_kernel(kbuf, block, jitter):
+    # the camera forward in packed passes (every pass splits: regroup_min=1) against the
+    # single camera kernel, on a faint cloud where rays need many gather rounds
+    dev = _dev()
+    sc = S.uniform_scene(20_000, 2, 61)
+    sc.density[:] = sc.density * 0.02
+    t = lambda a: torch.tensor(np.ascontiguousarray(a), device=dev)
+    scene = T.Scene(t(sc.mean), t(sc.scale), t(sc.quat), t(sc.density), t(sc.features))
+    cam = _camera(70, 45, eye=(2.0, -2.0, 1.2), fov=40.0)
+    jit = _jitter(cam, dev, jitter)
+    tune = T.Tune(kbuf, block, 0, regroup_min=1)
+    a = CAM.forward(scene, cam, jit, 0.0, 1000.0, 500, touch_count=True, ray_stats=True, tune=tune, regrouped=False)
+    b = CAM.forward(scene, cam, jit, 0.0, 1000.0, 500, touch_count=True, ray_stats=True, tune=tune, regrouped=True)
+    for k in ("out", "states", "last_dirac", "iters", "ray_stats", "touch_count", "status"):
+        assert torch.equal(getattr(a, k), getattr(b, k)), k
+    assert torch.equal(CAM.tri_collection(scene, cam, a, 500), CAM.tri_collection(scene, cam, b, 500))
+    assert int(a.iters.max()) > 2 * kbuf
