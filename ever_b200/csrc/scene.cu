@@ -6,6 +6,8 @@
 // cores, so the hierarchy is built here and traversed by our own kernels.
 #include <cstdio>
 
+#include <cuda/atomic>
+
 #include "common.cuh"
 #include "internal.cuh"
 
@@ -393,9 +395,11 @@ __global__ void k_refit(int64_t N, Node* __restrict__ nodes, const float4* __res
   if (j >= N) return;
   int n = parent_leaf[j];
   while (n >= 0) {
-    __threadfence();
-    if (atomicAdd(&flags[n], 1u) == 0u) return;  // the sibling subtree is not done yet
-    __threadfence();
+    // acquire-release at device scope: this thread's box stores above happen before the
+    // sibling's loads once it sees the count, and the sibling's stores before this thread's
+    // loads below (one instruction instead of two full fences around the atomic)
+    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> f(flags[n]);
+    if (f.fetch_add(1u, cuda::memory_order_acq_rel) == 0u) return;  // the sibling subtree is not done yet
     const int4 ch = __ldcg(&nodes[n].d);
     float3 l0, h0, l1, h1;
     child_box(nodes, aabb, ch.x, l0, h0);
