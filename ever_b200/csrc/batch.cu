@@ -37,11 +37,10 @@ BatchLayout batch_layout(int num_scenes, const EverBatchView* views, int num_vie
   return L;
 }
 
+// sh_degree < 0: the reference's DC-only forward colour (as ever_trace_forward)
 int degree_of(int K, int sh_degree) {
-  if (sh_degree >= 0) return sh_degree;
-  int k = 0;
-  while ((k + 1) * (k + 1) <= K) ++k;
-  return k - 1;
+  (void)K;
+  return sh_degree >= 0 ? sh_degree : 0;
 }
 
 EverTune tune_of(const EverTune* t) {

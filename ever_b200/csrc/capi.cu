@@ -35,14 +35,12 @@ EverTune resolve_tune(const EverTune* t) {
   return r;
 }
 
+// sh_degree < 0: the reference's forward colour, the DC term of every ellipsoid whatever
+// its SH size (shaders.slang:72-75, eval_sh_col0); 0..3: SH of that degree along rayd.
 int resolve_degree(const EverScene* sc, const EverTraceArgs* a, int* deg) {
   int d = a->sh_degree;
-  if (d < 0) {
-    int k = 0;
-    while ((k + 1) * (k + 1) <= sc->sh_coeffs) ++k;  // int(sqrt(K)), py_binding.cpp:206
-    d = k - 1;
-  }
-  if (d < 0 || d > 3) return fail(EVER_ERR_INVALID, "sh_degree %d out of range 0..3", d);
+  if (d < 0) d = 0;
+  if (d > 3) return fail(EVER_ERR_INVALID, "sh_degree %d out of range 0..3", d);
   if ((d + 1) * (d + 1) > sc->sh_coeffs)
     return fail(EVER_ERR_INVALID, "sh_degree %d needs %d SH coefficients, features have %d", d, (d + 1) * (d + 1),
                 sc->sh_coeffs);
@@ -221,7 +219,8 @@ int trace_backward(const EverScene* scene, const float* rayo, const float* rayd,
   float* acc_geo = reinterpret_cast<float*>(ws + c.take(N * 16 * sizeof(float)));
   float* acc_feat = reinterpret_cast<float*>(ws + c.take(N * int64_t(ever::feat_stride(scene->sh_coeffs)) * sizeof(float)));
   cudaError_t e = cudaSuccess;
-  if (N > 0) e = cudaMemsetAsync(workspace, 0, need, st);
+  // degree 0 keeps its DC feature gradients in the geometry rows: only those are cleared
+  if (N > 0) e = cudaMemsetAsync(workspace, 0, deg == 0 ? size_t(N) * 16 * sizeof(float) : need, st);
   if (e != cudaSuccess) return cuda_status(e, "ever_trace_backward memset");
   const bool per_ray_wct = wct && num_wct > 1 && out->dmeans2d;
   if (per_ray_wct && N > 0) {
@@ -269,6 +268,7 @@ int trace_backward(const EverScene* scene, const float* rayo, const float* rayd,
     F.quat = quat;
     F.acc_geo = acc_geo;
     F.acc_feat = acc_feat;
+    F.dc_only = deg == 0;
     F.wct = wct;
     F.num_wct = wct ? num_wct : 0;
     F.out = *out;

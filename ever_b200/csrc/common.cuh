@@ -70,11 +70,18 @@ __device__ __forceinline__ float3 rotate_vector(float3 v, float4 q) {
 }
 
 // Intersection record of one ellipsoid, 64 B: rows of W = diag(1/s) A(q) with the mean
-// in .w, then (density, original index bits, 0, 0). W (x - mean) are the unit-sphere
-// coordinates of x, i.e. rotate_vector(x - mean, q) / s (tri-intersect.slang:164-175).
+// in .w, then (density, DC colour). W (x - mean) are the unit-sphere coordinates of x,
+// i.e. rotate_vector(x - mean, q) / s (tri-intersect.slang:164-175). The DC colour is
+// C0 * f0 + 0.5 per channel (eval_sh_col0, sh.slang:49-51): the colour the reference's
+// forward gives every event (shaders.slang:72-75), so degree-0 traces read no feature row.
+// The original index of position j is the scene's order[j].
 struct __align__(16) Record {
   float4 r0, r1, r2, r3;
 };
+
+// The DC colour held in a record's r3 (the same bits as sh_colour<0> of the feature row).
+__device__ __forceinline__ float3 dc_colour(float4 r3) { return make_float3(r3.y, r3.z, r3.w); }
+__device__ __forceinline__ float dc_channel(float f0) { return fmaf(kShC0, f0, 0.5f); }
 
 struct __align__(16) Node {
   float4 a;  // child0 lo.xyz, hi.x

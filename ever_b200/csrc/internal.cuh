@@ -193,7 +193,7 @@ struct BwdParams {
   int log_cap;
   const float* wct;
   int num_wct;
-  float* acc_geo;   // N x 16 (W 9, mean 3, density 1, pad 3), Morton order
+  float* acc_geo;   // N x 16 (W 9, mean 3, density 1, DC feature gradient 3 at degree 0), Morton order
   float* acc_feat;  // N x K x 3, Morton order
   float* dmeans2d;  // per-ray wct mode accumulates here directly (original order)
   float* drayo;
@@ -212,6 +212,7 @@ struct FinalizeParams {
   const float* quat;
   const float* acc_geo;
   const float* acc_feat;
+  bool dc_only;      // degree-0 trace: acc_feat was neither cleared nor written (not read)
   const float* wct;  // first matrix, for the single-camera dmeans2d
   int num_wct;
   EverBackwardOut out;

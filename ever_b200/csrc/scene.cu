@@ -48,10 +48,13 @@ __device__ __forceinline__ float4 ld4(const float* p, int64_t i) {
   return make_float4(p[4 * i], p[4 * i + 1], p[4 * i + 2], p[4 * i + 3]);
 }
 
-// Conservative AABB of {x : |W (x - mean)| <= 1}: half extent i = |row_i(W^-1)|, computed
-// in double from the same W the intersection uses, then padded so that event times
-// computed in float never fall outside the box (grazing roots move by ~sqrt(eps) of the
-// radius).
+// Conservative AABB of {x : |W (x - mean)| <= 1}: half extent i = |row_i(W^-1)|, from the
+// same float W the intersection uses. W^-1 = adj(W) / det(W) is evaluated in float next to
+// a running bound of its rounding error (each 2x2 minor a*b - c*d is off by at most
+// 2u(|ab| + |cd|), u = 2^-24; det by the first row's share of those plus its own sums), and
+// the box is padded by that bound twice over, by 2e-3 of the extent (grazing roots in float
+// move by ~sqrt(u) of the radius) and by 4e-7 of the magnitudes, then rounded outwards.
+// Ill-conditioned W (det not known to 25%) gets an unbounded box. No double precision.
 __global__ void k_aabbs(const float* __restrict__ mean, const float* __restrict__ scale,
                         const float* __restrict__ quat, int64_t N, float4* __restrict__ aabb,
                         uint32_t* __restrict__ bounds) {
@@ -59,43 +62,69 @@ __global__ void k_aabbs(const float* __restrict__ mean, const float* __restrict_
   float3 c = make_float3(0.f, 0.f, 0.f);
   bool valid = false;
   if (p < N) {
-    float W[9];
-    prim_matrix(ld4(quat, p), ld3(scale, p), W);
+    float m[9];
+    prim_matrix(ld4(quat, p), ld3(scale, p), m);
     const float3 mu = ld3(mean, p);
-    double m[9];
-    for (int i = 0; i < 9; ++i) m[i] = W[i];
-    const double c00 = m[4] * m[8] - m[5] * m[7], c01 = m[5] * m[6] - m[3] * m[8], c02 = m[3] * m[7] - m[4] * m[6];
-    const double det = m[0] * c00 + m[1] * c01 + m[2] * c02;
+    constexpr float u = 5.9604645e-8f;  // 2^-24
+    // adjugate (rows of the inverse times det) and the sums of |products| of each minor
+    float adj[9], mag[9];
+    auto minor = [](float a, float b, float cc, float d, float& v, float& g) {
+      const float x = a * b, y = cc * d;
+      v = x - y;
+      g = fabsf(x) + fabsf(y);
+    };
+    minor(m[4], m[8], m[5], m[7], adj[0], mag[0]);
+    minor(m[2], m[7], m[1], m[8], adj[1], mag[1]);
+    minor(m[1], m[5], m[2], m[4], adj[2], mag[2]);
+    minor(m[5], m[6], m[3], m[8], adj[3], mag[3]);
+    minor(m[0], m[8], m[2], m[6], adj[4], mag[4]);
+    minor(m[2], m[3], m[0], m[5], adj[5], mag[5]);
+    minor(m[3], m[7], m[4], m[6], adj[6], mag[6]);
+    minor(m[1], m[6], m[0], m[7], adj[7], mag[7]);
+    minor(m[0], m[4], m[1], m[3], adj[8], mag[8]);
+    // det along the first row, with cofactors adj[0], adj[3], adj[6]
+    const float d0 = m[0] * adj[0], d1 = m[1] * adj[3], d2 = m[2] * adj[6];
+    const float det = (d0 + d1) + d2;
+    const float det_err = 3.f * u * (fabsf(m[0]) * mag[0] + fabsf(m[1]) * mag[3] + fabsf(m[2]) * mag[6]) +
+                          3.f * u * (fabsf(d0) + fabsf(d1) + fabsf(d2));
     float3 lo, hi;
     bool finite = isfinite(mu.x) && isfinite(mu.y) && isfinite(mu.z);
-    for (int i = 0; i < 9; ++i) finite = finite && isfinite(W[i]);
+    for (int i = 0; i < 9; ++i) finite = finite && isfinite(m[i]);
+    const float adet = fabsf(det);
     if (!finite) {
       // a degenerate far-away point: the slab test never reports it below tmax (and the
       // intersection of a non-finite ellipsoid yields no events anyway)
       lo = make_float3(3e38f, 3e38f, 3e38f);
       hi = lo;
-    } else if (!(fabs(det) > 1e-30) || !isfinite(det)) {
+    } else if (!(adet > 1e-30f) || !isfinite(det) || !(det_err < 0.25f * adet)) {
       lo = make_float3(-3e38f, -3e38f, -3e38f);
       hi = make_float3(3e38f, 3e38f, 3e38f);
     } else {
-      // inverse = adj / det, rows of the inverse
-      const double inv[9] = {c00 / det, (m[2] * m[7] - m[1] * m[8]) / det, (m[1] * m[5] - m[2] * m[4]) / det,
-                             c01 / det, (m[0] * m[8] - m[2] * m[6]) / det, (m[2] * m[3] - m[0] * m[5]) / det,
-                             c02 / det, (m[1] * m[6] - m[0] * m[7]) / det, (m[0] * m[4] - m[1] * m[3]) / det};
-      double e[3];
-      for (int i = 0; i < 3; ++i)
-        e[i] = sqrt(inv[3 * i] * inv[3 * i] + inv[3 * i + 1] * inv[3 * i + 1] + inv[3 * i + 2] * inv[3 * i + 2]);
-      const double mv[3] = {mu.x, mu.y, mu.z};
-      double l[3], h[3];
+      const float rel = det_err / (adet - det_err);  // relative error of 1/|det|
+      const float mv[3] = {mu.x, mu.y, mu.z};
+      float l[3], h[3];
+      bool ok = true;
       for (int i = 0; i < 3; ++i) {
-        const double pad = 2e-3 * e[i] + 4e-7 * (fabs(mv[i]) + e[i]) + 1e-30;
-        l[i] = mv[i] - e[i] - pad;
-        h[i] = mv[i] + e[i] + pad;
+        const float a0 = adj[3 * i], a1 = adj[3 * i + 1], a2 = adj[3 * i + 2];
+        const float g0 = mag[3 * i], g1 = mag[3 * i + 1], g2 = mag[3 * i + 2];
+        const float na = sqrtf(a0 * a0 + a1 * a1 + a2 * a2);
+        const float ng = sqrtf(g0 * g0 + g1 * g1 + g2 * g2);
+        const float e = na / adet;
+        const float err = e * (rel + 8.f * u) + 2.f * u * ng / adet * (1.f + rel);
+        const float pad = 2e-3f * e + 2.f * err + 4e-7f * (fabsf(mv[i]) + e) + 1e-30f;
+        ok = ok && isfinite(e) && isfinite(pad);
+        l[i] = __fsub_rd(__fsub_rd(mv[i], e), pad);
+        h[i] = __fadd_ru(__fadd_ru(mv[i], e), pad);
       }
-      lo = make_float3(__double2float_rd(l[0]), __double2float_rd(l[1]), __double2float_rd(l[2]));
-      hi = make_float3(__double2float_ru(h[0]), __double2float_ru(h[1]), __double2float_ru(h[2]));
-      c = make_float3(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z));
-      valid = isfinite(c.x) && isfinite(c.y) && isfinite(c.z);
+      if (ok) {
+        lo = make_float3(l[0], l[1], l[2]);
+        hi = make_float3(h[0], h[1], h[2]);
+        c = make_float3(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z));
+        valid = isfinite(c.x) && isfinite(c.y) && isfinite(c.z);
+      } else {
+        lo = make_float3(-3e38f, -3e38f, -3e38f);
+        hi = make_float3(3e38f, 3e38f, 3e38f);
+      }
     }
     aabb[2 * p] = make_float4(lo.x, lo.y, lo.z, 0.f);
     aabb[2 * p + 1] = make_float4(hi.x, hi.y, hi.z, 0.f);
@@ -300,18 +329,22 @@ __global__ void k_gather(const uint32_t* __restrict__ sorted_vals, int64_t N, in
   R.r0 = make_float4(W[0], W[1], W[2], mu.x);
   R.r1 = make_float4(W[3], W[4], W[5], mu.y);
   R.r2 = make_float4(W[6], W[7], W[8], mu.z);
-  R.r3 = make_float4(density[p], __int_as_float(int(p)), 0.f, 0.f);
-  recs[j] = R;
+  // r3.yzw (the DC colour) is written by k_gather_features, and kept by a refit without features
+  float4* rp = reinterpret_cast<float4*>(recs + j);
+  rp[0] = R.r0;
+  rp[1] = R.r1;
+  rp[2] = R.r2;
+  recs[j].r3.x = density[p];
   aabb_out[2 * j] = aabb_in[2 * p];
   aabb_out[2 * j + 1] = aabb_in[2 * p + 1];
 }
 
-// Feature rows into Morton order, one thread per padded float (coalesced on both sides).
 // Feature rows to Morton order, padded to feat_stride(K): one row per threadIdx.y, one
 // float4 column per threadIdx.x (blockDim.x = feat_stride(K) / 4), so no index division per
 // element. vec: the source rows are whole, 16-byte aligned float4s (3K % 4 == 0, aligned base).
+// Column 0 also writes the record's DC colour C0 * f0 + 0.5 (r3.yzw).
 __global__ void k_gather_features(const int32_t* __restrict__ order, int64_t N, int K, const float* __restrict__ feat,
-                                  float* __restrict__ feat_out, bool vec) {
+                                  float* __restrict__ feat_out, Record* __restrict__ recs, bool vec) {
   const int64_t j = int64_t(blockIdx.x) * blockDim.y + threadIdx.y;
   if (j >= N) return;
   const int c = threadIdx.x, per = 3 * K;
@@ -326,6 +359,11 @@ __global__ void k_gather_features(const int32_t* __restrict__ order, int64_t N, 
     v = make_float4(t[0], t[1], t[2], t[3]);
   }
   reinterpret_cast<float4*>(feat_out + j * feat_stride(K))[c] = v;
+  if (c == 0) {
+    recs[j].r3.y = dc_channel(v.x);
+    recs[j].r3.z = dc_channel(v.y);
+    recs[j].r3.w = dc_channel(v.z);
+  }
 }
 
 // Karras 2012: delta(i, j) = common prefix length of keys i, j (index bits break ties).
@@ -423,11 +461,12 @@ __global__ void k_single_leaf(Node* nodes, const float4* aabb) {
 
 inline int64_t div_up(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
-void launch_gather_features(const int32_t* order, int64_t N, int K, const float* feat, float* feat_out,
+void launch_gather_features(const int32_t* order, int64_t N, int K, const float* feat, float* feat_out, void* recs,
                             cudaStream_t st) {
   const int cols = feat_stride(K) / 4, rows = std::max(1, 256 / cols);
   const bool vec = (3 * K) % 4 == 0 && reinterpret_cast<uintptr_t>(feat) % 16 == 0;
-  k_gather_features<<<unsigned(div_up(N, rows)), dim3(cols, rows), 0, st>>>(order, N, K, feat, feat_out, vec);
+  k_gather_features<<<unsigned(div_up(N, rows)), dim3(cols, rows), 0, st>>>(order, N, K, feat, feat_out,
+                                                                           static_cast<Record*>(recs), vec);
 }
 
 }  // namespace
@@ -513,7 +552,7 @@ cudaError_t scene_build(const float* mean, const float* scale, const float* quat
   sort_pairs(ka, va, kb, vb, hist, N, 30, st);
   k_gather<<<unsigned(gb), tb, 0, st>>>(va, N, K, mean, scale, quat, density, aabb_a, aabb_b,
                                         reinterpret_cast<Record*>(sc->records), sc->features, sc->order);
-  launch_gather_features(sc->order, N, K, feat, sc->features, st);
+  launch_gather_features(sc->order, N, K, feat, sc->features, sc->records, st);
   if (N == 1) {
     k_single_leaf<<<1, 1, 0, st>>>(nodes, aabb_b);
     return cudaGetLastError();
@@ -547,7 +586,7 @@ cudaError_t scene_refit(const float* mean, const float* scale, const float* quat
                                         aabb_a, aabb_b, reinterpret_cast<Record*>(sc->records), sc->features,
                                         sc->order);
   if (feat)
-    launch_gather_features(sc->order, N, K, feat, sc->features, st);
+    launch_gather_features(sc->order, N, K, feat, sc->features, sc->records, st);
   if (N == 1) {
     k_single_leaf<<<1, 1, 0, st>>>(nodes, aabb_b);
     return cudaGetLastError();
@@ -561,7 +600,7 @@ cudaError_t scene_refit(const float* mean, const float* scale, const float* quat
 cudaError_t scene_set_features(EverScene* sc, const float* feat, cudaStream_t st) {
   const int64_t total = sc->num_prims * int64_t(sc->sh_coeffs) * 3;
   if (total == 0) return cudaSuccess;
-  launch_gather_features(sc->order, sc->num_prims, sc->sh_coeffs, feat, sc->features, st);
+  launch_gather_features(sc->order, sc->num_prims, sc->sh_coeffs, feat, sc->features, sc->records, st);
   return cudaGetLastError();
 }
 

@@ -54,7 +54,7 @@ __device__ __forceinline__ Ctrl load_ctrl(const Record* recs, const float* feats
   HitT H;
   intersect(R, ray, H);
   c.t = c.entry ? H.t0 : H.t1;
-  c.c = sh_colour<DEG>(feats + c.j * fstride, B);
+  c.c = DEG == 0 ? dc_colour(R.r3) : sh_colour<DEG>(feats + c.j * fstride, B);
   const float dh = c.entry ? R.r3.x : -R.r3.x;
   c.dirac = make_float4(dh, dh * c.c.x, dh * c.c.y, dh * c.c.z);
   return c;
@@ -228,6 +228,7 @@ struct BScene {
   const Node* nodes;
   const Record* recs;
   const float* features;
+  const int32_t* order;  // Morton position -> original index
   int K;
   float* acc_geo;
   float* acc_feat;
@@ -482,7 +483,16 @@ __device__ void backward_ray(const BScene& S, const BRayCtx& P, int64_t r, int64
     const Record R = load_record(recs, j);
     const float sign = cur.entry ? 1.f : -1.f;
     float gc[3];
-    const float g_sigma = colour_coeffs<DEG>(S, j, sign * R.r3.x, sign, cur.c, Gd, GB, gc);
+    float g_sigma;
+    if (DEG == 0) {  // the DC colour: no feature row, no direction gradient
+      const float dh = sign * R.r3.x;
+      g_sigma = sign * (Gd.x + Gd.y * cur.c.x + Gd.z * cur.c.y + Gd.w * cur.c.z);
+      gc[0] = dh * Gd.y;
+      gc[1] = dh * Gd.z;
+      gc[2] = dh * Gd.w;
+    } else {
+      g_sigma = colour_coeffs<DEG>(S, j, sign * R.r3.x, sign, cur.c, Gd, GB, gc);
+    }
     // event time: root of |ocn + t rdn|^2 = 1. dt = -(P.docn + t P.drdn) / (P.rdn) with the
     // hit point in the cancellation-free form P = l +- (sqrt(h)/a) rdn and P.rdn = +-sqrt(h)
     FullHit H;
@@ -532,7 +542,7 @@ __device__ void backward_ray(const BScene& S, const BRayCtx& P, int64_t r, int64
         const float mx = R.r0.w, my = R.r1.w, mz = R.r2.w;
         const float z = mx * wct[2] + my * wct[6] + mz * wct[10] + wct[14];
         const float gm[3] = {-gmu[0], -gmu[1], -gmu[2]};
-        const int p = __float_as_int(R.r3.y);
+        const int p = __ldg(S.order + j);
         const float dx = z * (iwct[0] * gm[0] + iwct[1] * gm[1] + iwct[2] * gm[2]);
         const float dy = z * (iwct[4] * gm[0] + iwct[5] * gm[1] + iwct[6] * gm[2]);
         atomicAdd(reinterpret_cast<float2*>(P.dmeans2d) + p, make_float2(dx, dy));
@@ -542,9 +552,14 @@ __device__ void backward_ray(const BScene& S, const BRayCtx& P, int64_t r, int64
     atomicAdd(ag + 0, make_float4(gW[0], gW[1], gW[2], gW[3]));
     atomicAdd(ag + 1, make_float4(gW[4], gW[5], gW[6], gW[7]));
     atomicAdd(ag + 2, make_float4(gW[8], -gmu[0], -gmu[1], -gmu[2]));
-    atomicAdd(ag + 3, make_float4(g_sigma, 0.f, 0.f, 0.f));
-    const float ev[kGradRow] = {gc[0], gc[1], gc[2]};
-    pending_add<DEG>(S, B, pj, acc, j, cur.entry, ev);
+    if (DEG == 0) {
+      // degree 0: the DC feature gradient B_0 gc rides in the row's three pad floats
+      atomicAdd(ag + 3, make_float4(g_sigma, B[0] * gc[0], B[0] * gc[1], B[0] * gc[2]));
+    } else {
+      atomicAdd(ag + 3, make_float4(g_sigma, 0.f, 0.f, 0.f));
+      const float ev[kGradRow] = {gc[0], gc[1], gc[2]};
+      pending_add<DEG>(S, B, pj, acc, j, cur.entry, ev);
+    }
     s = so;
     G = Gs;
     G.t = Gs.t;
@@ -576,9 +591,18 @@ __device__ void backward_ray(const BScene& S, const BRayCtx& P, int64_t r, int64
           const Record R = load_record(recs, j);
           HitT H;
           if (intersect(R, ray, H) && H.t0 <= 0.f && H.t1 > 0.f) {
-            const float3 col = sh_colour<DEG>(S.features + j * fstride, B);
-            const float g_sigma = colour_grads<DEG>(S, j, R.r3.x, 1.f, col, G.drgb, B, GB);
-            atomicAdd(S.acc_geo + int64_t(j) * kGeo + 12, g_sigma);
+            if (DEG == 0) {
+              const float3 col = dc_colour(R.r3);
+              const float4 Gd = G.drgb;
+              const float dh = R.r3.x;
+              const float g_sigma = Gd.x + Gd.y * col.x + Gd.z * col.y + Gd.w * col.z;
+              atomicAdd(reinterpret_cast<float4*>(S.acc_geo + int64_t(j) * kGeo) + 3,
+                        make_float4(g_sigma, B[0] * (dh * Gd.y), B[0] * (dh * Gd.z), B[0] * (dh * Gd.w)));
+            } else {
+              const float3 col = sh_colour<DEG>(S.features + j * fstride, B);
+              const float g_sigma = colour_grads<DEG>(S, j, R.r3.x, 1.f, col, G.drgb, B, GB);
+              atomicAdd(S.acc_geo + int64_t(j) * kGeo + 12, g_sigma);
+            }
           }
         }
       }
@@ -625,8 +649,8 @@ __global__ void __launch_bounds__(256, 2) k_trace_bwd(const BwdParams P) {
   if (gi >= P.R) return;
   const int64_t slot = P.slot_order ? int64_t(P.slot_order[gi]) : gi;  // event-log column
   const int64_t r = P.ray_order ? int64_t(P.ray_order[slot]) : slot;
-  const BScene S{reinterpret_cast<const Node*>(P.nodes), reinterpret_cast<const Record*>(P.records), P.features, P.K,
-                 P.acc_geo, P.acc_feat};
+  const BScene S{reinterpret_cast<const Node*>(P.nodes), reinterpret_cast<const Record*>(P.records), P.features,
+                 P.order, P.K, P.acc_geo, P.acc_feat};
   const BRayCtx C{P.rayo, P.rayd, P.tmin, P.max_iters, P.grad_out, P.states, P.iters, P.event_log, P.R,
                   P.drayo, P.drayd, P.wct, P.num_wct, P.dmeans2d};
   backward_ray<DEG>(S, C, r, slot, load3(P.rayo, r), load3(P.rayd, r));
@@ -643,8 +667,8 @@ __global__ void __launch_bounds__(256, 2)
   const int64_t slot = P.slot_order ? int64_t(P.slot_order[gi]) : gi;
   const int64_t p = camera_slot_pixel(cam, slot);
   if (p < 0) return;
-  const BScene S{reinterpret_cast<const Node*>(P.nodes), reinterpret_cast<const Record*>(P.records), P.features, P.K,
-                 P.acc_geo, P.acc_feat};
+  const BScene S{reinterpret_cast<const Node*>(P.nodes), reinterpret_cast<const Record*>(P.records), P.features,
+                 P.order, P.K, P.acc_geo, P.acc_feat};
   const BRayCtx C{nullptr, nullptr, P.tmin, P.max_iters, P.grad_out, P.states, P.iters, P.event_log, P.R,
                   P.drayo, P.drayd, P.wct, P.num_wct, P.dmeans2d};
   float3 ro, rd;
@@ -678,7 +702,7 @@ __global__ void __launch_bounds__(256, 2) k_trace_bwd_batched(const BatchBwdPara
     const int v = lo;
     const BatchScene bs_ = P.scenes[P.views[v].scene];
     const BScene S{reinterpret_cast<const Node*>(bs_.nodes), reinterpret_cast<const Record*>(bs_.records),
-                   bs_.features, bs_.K, bs_.acc_geo, bs_.acc_feat};
+                   bs_.features, bs_.order, bs_.K, bs_.acc_geo, bs_.acc_feat};
     const int32_t r = P.slot_ray[slot];
     if (r >= 0) backward_ray<DEG>(S, C, r, slot, load3(P.rayo, r), load3(P.rayd, r));
     __syncwarp();
@@ -745,13 +769,23 @@ __global__ void k_finalize(const FinalizeParams P) {
 
 // Feature gradients back to original order and shape (N,K,3), clipped at 1e3: one row per
 // threadIdx.y, one float4 column per threadIdx.x (blockDim.x = feat_stride(K) / 4). vec: the
-// output rows are whole, 16-byte aligned float4s (3K % 4 == 0, aligned base).
+// output rows are whole, 16-byte aligned float4s (3K % 4 == 0, aligned base). The DC
+// gradient of degree-0 traces sits in the pad floats 13..15 of the geometry row and is
+// added to coefficient 0; dc_only: the feature rows were not used (all zero, not read).
 __global__ void k_finalize_features(const int32_t* __restrict__ order, int64_t N, int K,
-                                    const float* __restrict__ acc_feat, float* __restrict__ dfeat, bool vec) {
+                                    const float* __restrict__ acc_feat, const float* __restrict__ acc_geo,
+                                    bool dc_only, float* __restrict__ dfeat, bool vec) {
   const int64_t j = int64_t(blockIdx.x) * blockDim.y + threadIdx.y;
   if (j >= N) return;
   const int c = threadIdx.x, per = 3 * K;
-  const float4 a = reinterpret_cast<const float4*>(acc_feat + j * feat_stride(K))[c];
+  float4 a = dc_only ? make_float4(0.f, 0.f, 0.f, 0.f)
+                     : reinterpret_cast<const float4*>(acc_feat + j * feat_stride(K))[c];
+  if (c == 0) {
+    const float* g = acc_geo + j * kGeo;
+    a.x += g[13];
+    a.y += g[14];
+    a.z += g[15];
+  }
   const float4 g = make_float4(clip_grad(a.x, 1e3f), clip_grad(a.y, 1e3f), clip_grad(a.z, 1e3f), clip_grad(a.w, 1e3f));
   float* dst = dfeat + int64_t(__ldg(order + j)) * per;
   if (vec) {
@@ -880,8 +914,8 @@ cudaError_t launch_finalize(const FinalizeParams& P, cudaStream_t st) {
   k_finalize<<<unsigned((P.N + 255) / 256), 256, 0, st>>>(P);
   const int cols = feat_stride(P.K) / 4, rows = 256 / cols > 0 ? 256 / cols : 1;
   const bool vec = (3 * P.K) % 4 == 0 && reinterpret_cast<uintptr_t>(P.out.dfeatures) % 16 == 0;
-  k_finalize_features<<<unsigned((P.N + rows - 1) / rows), dim3(cols, rows), 0, st>>>(P.order, P.N, P.K, P.acc_feat,
-                                                                                     P.out.dfeatures, vec);
+  k_finalize_features<<<unsigned((P.N + rows - 1) / rows), dim3(cols, rows), 0, st>>>(
+      P.order, P.N, P.K, P.acc_feat, P.acc_geo, P.dc_only, P.out.dfeatures, vec);
   return cudaGetLastError();
 }
 

@@ -217,19 +217,19 @@ __device__ __forceinline__ void member_insert(int p, int j, int& n_mem, int (&me
 // Ellipsoid j contains the ray start (t0 <= 0 < t1): record it (sorted by original index);
 // beyond kMaxMembers the rest are summed into `extra` in traversal order (status flag).
 template <int DEG>
-__device__ __forceinline__ void point_leaf(const Record* __restrict__ recs, const float* __restrict__ feats, int fst,
-                                           const float* B, int bs, const Ray& ray, int j, int& n_mem,
-                                           int (&mem_p)[kMaxMembers], int (&mem_j)[kMaxMembers], float4& extra,
-                                           uint32_t& status) {
+__device__ __forceinline__ void point_leaf(const Record* __restrict__ recs, const int32_t* __restrict__ order,
+                                           const float* __restrict__ feats, int fst, const float* B, int bs,
+                                           const Ray& ray, int j, int& n_mem, int (&mem_p)[kMaxMembers],
+                                           int (&mem_j)[kMaxMembers], float4& extra, uint32_t& status) {
   const Record R = load_record(recs, j);
   HitT H;
   if (!(intersect(R, ray, H) && H.t0 <= 0.f && H.t1 > 0.f)) return;
   if (n_mem < kMaxMembers) {
-    member_insert(__float_as_int(R.r3.y), j, n_mem, mem_p, mem_j);
+    member_insert(__ldg(order + j), j, n_mem, mem_p, mem_j);
   } else {
     status |= EVER_STATUS_INIT_OVERFLOW;
     const float sg = R.r3.x;
-    const float3 c = sh_colour<DEG>(feats + int64_t(j) * fst, B, bs);
+    const float3 c = DEG == 0 ? dc_colour(R.r3) : sh_colour<DEG>(feats + int64_t(j) * fst, B, bs);
     extra.x = extra.x + sg;
     extra.y = extra.y + sg * c.x;
     extra.z = extra.z + sg * c.y;
@@ -240,7 +240,8 @@ __device__ __forceinline__ void point_leaf(const Record* __restrict__ recs, cons
 // Point query for the ray start; PACKET: warp-uniform walk.
 template <int DEG, bool PACKET>
 __device__ int point_members(const Node* __restrict__ nodes, const Record* __restrict__ recs,
-                             const float* __restrict__ feats, int fst, const float* B, int bs, const Ray& ray, bool act,
+                             const int32_t* __restrict__ order, const float* __restrict__ feats, int fst,
+                             const float* B, int bs, const Ray& ray, bool act,
                              int* stack, int stride, int lane, int (&mem_p)[kMaxMembers], int (&mem_j)[kMaxMembers],
                              float4& extra, uint32_t& status) {
   int n_mem = 0;
@@ -251,8 +252,8 @@ __device__ int point_members(const Node* __restrict__ nodes, const Record* __res
     const bool h0 = act && box_contains(nd.a.x, nd.a.y, nd.a.z, nd.a.w, nd.b.x, nd.b.y, ray.o);
     const bool h1 = act && box_contains(nd.b.z, nd.b.w, nd.c.x, nd.c.y, nd.c.z, nd.c.w, ray.o);
     const int c0 = nd.d.x, c1 = nd.d.y;
-    if (h0 && c0 < 0) point_leaf<DEG>(recs, feats, fst, B, bs, ray, ~c0, n_mem, mem_p, mem_j, extra, status);
-    if (h1 && c1 < 0) point_leaf<DEG>(recs, feats, fst, B, bs, ray, ~c1, n_mem, mem_p, mem_j, extra, status);
+    if (h0 && c0 < 0) point_leaf<DEG>(recs, order, feats, fst, B, bs, ray, ~c0, n_mem, mem_p, mem_j, extra, status);
+    if (h1 && c1 < 0) point_leaf<DEG>(recs, order, feats, fst, B, bs, ray, ~c1, n_mem, mem_p, mem_j, extra, status);
     bool g0 = h0 && c0 >= 0, g1 = h1 && c1 >= 0;
     if (PACKET) {
       g0 = __any_sync(kFull, g0);
@@ -283,6 +284,7 @@ struct SceneRef {
   const Node* nodes;
   const Record* recs;
   const float* features;
+  const int32_t* order;  // Morton position -> original index
   int64_t N;
   int K;
 };
@@ -319,7 +321,7 @@ __device__ __forceinline__ bool consume(const SceneRef& sc, const TraceCtx& C, c
       intersect(load_record(sc.recs, j), ray, H);
       if (!(H.t0 > s16 && H.t0 <= C.tmax)) continue;
     }
-    const float3 c = sh_colour<DEG>(sc.features + int64_t(j) * fst, B, bs);
+    const float3 c = DEG == 0 ? dc_colour(r3) : sh_colour<DEG>(sc.features + int64_t(j) * fst, B, bs);
     const float dh = ex ? -r3.x : r3.x;
     const float4 dirac = make_float4(dh, dh * c.x, dh * c.y, dh * c.z);
     update(s, t, dirac);
@@ -330,7 +332,7 @@ __device__ __forceinline__ bool consume(const SceneRef& sc, const TraceCtx& C, c
       else
         status |= EVER_STATUS_LOG_OVERFLOW;
     }
-    if (C.out.touch_count) atomicAdd(C.out.touch_count + __float_as_int(r3.y), 1);
+    if (C.out.touch_count) atomicAdd(C.out.touch_count + __ldg(sc.order + j), 1);
     ++iters;
     if (++cnt16 == kRefRound) {
       s16 = t;
@@ -350,8 +352,9 @@ __device__ __forceinline__ void init_density(const SceneRef& sc, const float* B,
   const int fst = feat_stride(sc.K);
   for (int q = 0; q < n_mem; ++q) {
     const int j = mem_j[q];
-    const float sg = __ldg(&sc.recs[j].r3.x);
-    const float3 c = sh_colour<DEG>(sc.features + int64_t(j) * fst, B, bs);
+    const float4 r3 = __ldg(&sc.recs[j].r3);
+    const float sg = r3.x;
+    const float3 c = DEG == 0 ? dc_colour(r3) : sh_colour<DEG>(sc.features + int64_t(j) * fst, B, bs);
     s.drgb.x = s.drgb.x + sg;
     s.drgb.y = s.drgb.y + sg * c.x;
     s.drgb.z = s.drgb.z + sg * c.y;
@@ -397,7 +400,7 @@ __device__ __forceinline__ Ray load_ray(const float* rayo, const float* rayd, in
 
 __device__ __forceinline__ SceneRef scene_of(const FwdParams& P) {
   return SceneRef{reinterpret_cast<const Node*>(P.nodes), reinterpret_cast<const Record*>(P.records), P.features,
-                  P.N, P.K};
+                  P.order, P.N, P.K};
 }
 
 template <int KBUF, int DEG>
@@ -422,7 +425,8 @@ __global__ void __launch_bounds__(256) k_trace_fwd_ray(const FwdParams P) {
   if (sc.N > 0) {
     int mem_p[kMaxMembers], mem_j[kMaxMembers];
     float4 extra = make_float4(0.f, 0.f, 0.f, 0.f);
-    const int n_mem = point_members<DEG, false>(sc.nodes, sc.recs, sc.features, feat_stride(sc.K), B, 1, ray, true,
+    const int n_mem = point_members<DEG, false>(sc.nodes, sc.recs, sc.order, sc.features, feat_stride(sc.K), B, 1,
+                                                ray, true,
                                                 st_node, stride, 0, mem_p, mem_j, extra, status);
     init_density<DEG>(sc, B, 1, n_mem, mem_j, extra, status, s);
     float s16 = 0.f;
@@ -476,7 +480,8 @@ __device__ __forceinline__ RayLoop start_ray(const SceneRef& sc, const Ray& ray,
   if (sc.N > 0) {
     int mem_p[kMaxMembers], mem_j[kMaxMembers];
     float4 extra = make_float4(0.f, 0.f, 0.f, 0.f);
-    const int n_mem = point_members<DEG, true>(sc.nodes, sc.recs, sc.features, feat_stride(sc.K), B, bs, ray, valid,
+    const int n_mem = point_members<DEG, true>(sc.nodes, sc.recs, sc.order, sc.features, feat_stride(sc.K), B, bs,
+                                               ray, valid,
                                                wstack, 1, lane, mem_p, mem_j, extra, L.status);
     init_density<DEG>(sc, B, bs, n_mem, mem_j, extra, L.status, L.s);
   }
@@ -683,7 +688,7 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value) k_trace_fwd
     while (v + 1 < P.num_views && P.views[v + 1].slot_offset <= int64_t(pk) * 32) ++v;
     const BatchScene bs_ = P.scenes[P.views[v].scene];
     const SceneRef sc{reinterpret_cast<const Node*>(bs_.nodes), reinterpret_cast<const Record*>(bs_.records),
-                      bs_.features, bs_.N, bs_.K};
+                      bs_.features, bs_.order, bs_.N, bs_.K};
     const int32_t r = P.slot_ray[slot];
     const Ray ray = load_ray(P.rayo, P.rayd, r >= 0 ? r : 0, P.tmin);
     trace_packet<KBUF, DEG>(sc, C, ray, r, r >= 0, slot, wstack, B, blockDim.x, lane);

@@ -14,11 +14,16 @@ clipping. Everything runs in libever_b200.so: an LBVH built on the device per ca
 (the reference rebuilds its GAS per call as well, :66-71), a CUDA traversal/integration
 kernel and a CUDA reverse-replay backward.
 
-Colour: the SH degree is sqrt(K)-1 of features (N,K,3) as in py_binding.cpp:206 and the
-colour of each ellipsoid is evaluated along the ray direction rayd, as the reference's
-backward evaluates it (backwards_kernel.slang:162, 238). At degree 0 (the trainer's
-case) this equals the reference's forward, which reads only the DC term; pass
-sh_degree=0 to get that DC-only colour with higher-degree features too.
+Colour: by default (sh_degree=None) every event takes the ellipsoid's DC colour
+C0 * f0 + 0.5 whatever the size K of features (N,K,3), exactly as the reference's forward
+(shaders.slang:72-75: get_sh(sh_feats, 0), eval_sh_col0), and the backward differentiates
+that colour: feature gradients of the coefficients k >= 1 are zero. The reference's
+backward instead differentiates SH of degree sqrt(K)-1 along rayd
+(backwards_kernel.slang:162, 238) against the DC-built states, so for K > 1 its feature
+gradients are those of a colour its forward never computed; this drop-in returns the
+gradients of the image it returned. Opt in to view-dependent colour with sh_degree=d
+(1..3, needs (d+1)^2 <= K): SH of degree d evaluated along the raw ray direction rayd in
+both passes.
 
 Launch order: by default the rays are first sorted into a coherent order on the device
 (ray_order="auto", see ever_ray_order in include/ever_b200.h) so that each warp's packet

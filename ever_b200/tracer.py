@@ -126,6 +126,7 @@ class ForwardResult:
 
 
 def trace_args(tmin, tmax, max_iters, sh_degree):
+    """sh_degree None: the reference's DC-only forward colour; d: SH of degree d along rayd."""
     a = N.EverTraceArgs()
     a.tmin, a.tmax, a.max_iters = float(tmin), float(tmax), int(max_iters)
     a.sh_degree = -1 if sh_degree is None else int(sh_degree)

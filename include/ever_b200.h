@@ -97,7 +97,10 @@ typedef struct EverTraceArgs {
   float tmin;
   float tmax;
   int32_t max_iters;
-  int32_t sh_degree;  /* SH degree evaluated (0..3); -1: sqrt(K)-1 as py_binding.cpp:206 */
+  int32_t sh_degree;  /* colour of an event. -1 (default): the reference's forward colour,
+                         the ellipsoid's DC term C0*f0 + 0.5 whatever K (shaders.slang:72-75,
+                         eval_sh_col0), and its gradient in the backward (features k >= 1 get
+                         zero); 0..3: SH of that degree along the raw rayd in both passes */
 } EverTraceArgs;
 
 const char* ever_last_error(void);
@@ -262,8 +265,8 @@ int ever_batch_setup(const EverScene* scenes, void* const* bwd_workspaces, int32
 int ever_batch_order(const EverBatch* batch, const float* rayo, const float* rayd, void* stream);
 
 /* One persistent forward launch over all views. Outputs are indexed by ray; event_log
- * has log_cap rows of batch->num_slots columns. The scenes must share an SH degree
- * (args->sh_degree, or sqrt(K)-1 of the first scene). */
+ * has log_cap rows of batch->num_slots columns. The colour follows args->sh_degree as in
+ * ever_trace_forward; every scene must hold the coefficients it needs. */
 int ever_trace_forward_batched(const EverBatch* batch, const float* rayo, const float* rayd,
                                const EverTraceArgs* args, const EverTune* tune, const EverForwardOut* out,
                                void* stream);

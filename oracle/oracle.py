@@ -87,6 +87,13 @@ def sh_degree_of(K: int) -> int:
     return int(np.sqrt(K)) - 1
 
 
+def colour_degree(sh_degree) -> int:
+    """The SH degree the colour is evaluated at. None is the reference's forward: the DC
+    term of every ellipsoid whatever K (shaders.slang:72-75, get_sh(sh_feats, 0) and
+    eval_sh_col0), i.e. degree 0. An int d evaluates SH of degree d along rayd."""
+    return 0 if sh_degree is None else int(sh_degree)
+
+
 @dataclass
 class Trace:
     out: np.ndarray        # (R,5) RGB, opacity, distortion
@@ -104,7 +111,7 @@ def trace(scene: Scene, rayo, rayd, tmin=0.0, tmax=1000.0, max_iters=500, sh_deg
     rayo = np.ascontiguousarray(np.asarray(rayo, dtype=dt).reshape(-1, 3))
     rayd = np.ascontiguousarray(np.asarray(rayd, dtype=dt).reshape(-1, 3))
     R = rayo.shape[0]
-    deg = sh_degree_of(s.K) if sh_degree is None else int(sh_degree)
+    deg = colour_degree(sh_degree)
     out = np.zeros((R, 5), dt)
     states = np.zeros((R, 16), dt)
     last_dirac = np.zeros((R, 4), dt)
@@ -143,7 +150,7 @@ def backward(scene: Scene, rayo, rayd, tmin, tmax, max_iters, events, iters, dou
     rayo = np.ascontiguousarray(np.asarray(rayo, np.float64).reshape(-1, 3))
     rayd = np.ascontiguousarray(np.asarray(rayd, np.float64).reshape(-1, 3))
     R = rayo.shape[0]
-    deg = sh_degree_of(s.K) if sh_degree is None else int(sh_degree)
+    deg = colour_degree(sh_degree)
     events = np.ascontiguousarray(events, np.int32)
     iters = np.ascontiguousarray(iters, np.int32)
     dout = np.ascontiguousarray(np.asarray(dout, np.float64).reshape(R, 5))

@@ -19,7 +19,7 @@ def _dev():
     return torch.device("cuda:0")
 
 
-def _gpu_grads(sc, ro, rd, dout, tmin=0.0, tmax=1000.0, max_iters=500, wcts=None):
+def _gpu_grads(sc, ro, rd, dout, tmin=0.0, tmax=1000.0, max_iters=500, wcts=None, sh_degree=None):
     dev = _dev()
     t = {k: torch.tensor(np.ascontiguousarray(getattr(sc, k), np.float32), device=dev, requires_grad=True)
          for k in NAMES}
@@ -27,7 +27,7 @@ def _gpu_grads(sc, ro, rd, dout, tmin=0.0, tmax=1000.0, max_iters=500, wcts=None
     rayd = torch.tensor(np.asarray(rd, np.float32), device=dev, requires_grad=True)
     m2d = torch.zeros((sc.mean.shape[0], 2), device=dev, requires_grad=True) if wcts is not None else None
     out = trace_rays(t["mean"], t["scale"], t["quat"], t["density"], t["features"], rayo, rayd, tmin, tmax, 3,
-                     m2d, wcts, max_iters)
+                     m2d, wcts, max_iters, sh_degree=sh_degree)
     (out * torch.tensor(dout, dtype=torch.float32, device=dev)).sum().backward()
     g = {k: v.grad.cpu().double().numpy() for k, v in t.items()}
     g["rayo"] = rayo.grad.cpu().double().numpy()
@@ -37,10 +37,11 @@ def _gpu_grads(sc, ro, rd, dout, tmin=0.0, tmax=1000.0, max_iters=500, wcts=None
     return g, out.detach().cpu().numpy()
 
 
-def _oracle_grads(sc, ro, rd, dout, tmin=0.0, tmax=1000.0, max_iters=500, mode="f64"):
+def _oracle_grads(sc, ro, rd, dout, tmin=0.0, tmax=1000.0, max_iters=500, mode="f64", sh_degree=None):
     s = O.Scene(sc.mean, sc.scale, sc.quat, np.asarray(sc.density).reshape(-1), sc.features)
-    tr = O.trace(s, ro, rd, tmin, tmax, max_iters)  # float32 event sequence, as the GPU consumed it
-    g = O.backward(s, ro, rd, tmin, tmax, max_iters, tr.events, tr.iters, dout, mode=mode)
+    # float32 event sequence, as the GPU consumed it
+    tr = O.trace(s, ro, rd, tmin, tmax, max_iters, sh_degree)
+    g = O.backward(s, ro, rd, tmin, tmax, max_iters, tr.events, tr.iters, dout, sh_degree=sh_degree, mode=mode)
     return {"mean": g.mean, "scale": g.scale, "quat": g.quat, "density": g.density.reshape(-1, 1),
             "features": g.features, "rayo": g.rayo, "rayd": g.rayd}
 
@@ -64,14 +65,15 @@ REPLAY_TOL = 1e-4
 GRAD_TOL = 5e-3
 
 
-@pytest.mark.parametrize("deg,seed", [(0, 1), (3, 2)])
-def test_gradients_match_fp64_oracle(deg, seed):
+@pytest.mark.parametrize("deg,seed,sh_degree", [(0, 1, None), (3, 2, None), (3, 2, 3)])
+def test_gradients_match_fp64_oracle(deg, seed, sh_degree):
+    # sh_degree None: the reference's DC-only colour (the default); 3: view-dependent SH
     sc = S.uniform_scene(1500, deg, seed=seed)
     ro, rd = S.look_at_rays(S.Camera(np.array([0.0, 0.0, 3.0]), 24, 24, 50.0))
     dout = np.random.default_rng(seed).normal(size=(ro.shape[0], 5))
-    g, _ = _gpu_grads(sc, ro, rd, dout)
-    ref = _oracle_grads(sc, ro, rd, dout)
-    rep = _oracle_grads(sc, ro, rd, dout, mode="f32_replay")
+    g, _ = _gpu_grads(sc, ro, rd, dout, sh_degree=sh_degree)
+    ref = _oracle_grads(sc, ro, rd, dout, sh_degree=sh_degree)
+    rep = _oracle_grads(sc, ro, rd, dout, mode="f32_replay", sh_degree=sh_degree)
     for k in ref:
         assert _rel_err(g[k], _clip(k, rep[k])) < REPLAY_TOL, (k, _rel_err(g[k], _clip(k, rep[k])))
         assert _rel_err(g[k], _clip(k, ref[k])) < GRAD_TOL, (k, _rel_err(g[k], _clip(k, ref[k])))
@@ -93,9 +95,10 @@ def test_gradients_nested_ellipsoids():
     sc = S.SceneArrays(mean, scale, quat, density, features)
     ro, rd = S.look_at_rays(S.Camera(np.array([0.3, -0.2, 3.0]), 16, 16, 12.0))
     dout = rng.normal(size=(ro.shape[0], 5))
-    g, _ = _gpu_grads(sc, ro, rd, dout)
-    ref = _oracle_grads(sc, ro, rd, dout)
-    rep = _oracle_grads(sc, ro, rd, dout, mode="f32_replay")
+    # view-dependent SH: the pending rows hold SH-space colour gradients
+    g, _ = _gpu_grads(sc, ro, rd, dout, sh_degree=3)
+    ref = _oracle_grads(sc, ro, rd, dout, sh_degree=3)
+    rep = _oracle_grads(sc, ro, rd, dout, mode="f32_replay", sh_degree=3)
     tr = O.trace(O.Scene(mean, scale, quat, density.reshape(-1), features), ro, rd, 0.0, 1000.0, 500)
     assert tr.iters.max() >= 12  # rays cross most of the shells: many ellipsoids open at once
     for k in ref:
@@ -103,14 +106,15 @@ def test_gradients_nested_ellipsoids():
         assert _rel_err(g[k], _clip(k, ref[k])) < GRAD_TOL, (k, _rel_err(g[k], _clip(k, ref[k])))
 
 
-def test_gradients_rays_inside_and_tmin():
+@pytest.mark.parametrize("sh_degree", [None, 3])
+def test_gradients_rays_inside_and_tmin(sh_degree):
     sc = S.uniform_scene(1200, 3, seed=5)
     sc.scale *= 2.5
     ro, rd = S.look_at_rays(S.Camera(np.array([0.1, 0.0, 0.3]), 16, 16, 80.0))
     dout = np.random.default_rng(5).normal(size=(ro.shape[0], 5))
-    g, _ = _gpu_grads(sc, ro, rd, dout, tmin=0.05)
-    ref = _oracle_grads(sc, ro, rd, dout, tmin=0.05)
-    rep = _oracle_grads(sc, ro, rd, dout, tmin=0.05, mode="f32_replay")
+    g, _ = _gpu_grads(sc, ro, rd, dout, tmin=0.05, sh_degree=sh_degree)
+    ref = _oracle_grads(sc, ro, rd, dout, tmin=0.05, sh_degree=sh_degree)
+    rep = _oracle_grads(sc, ro, rd, dout, tmin=0.05, mode="f32_replay", sh_degree=sh_degree)
     for k in ref:
         assert _rel_err(g[k], _clip(k, rep[k])) < REPLAY_TOL, (k, _rel_err(g[k], _clip(k, rep[k])))
         assert _rel_err(g[k], _clip(k, ref[k])) < GRAD_TOL, (k, _rel_err(g[k], _clip(k, ref[k])))

@@ -67,6 +67,49 @@ def _worker(rank, world, port, mode, result_dir):
             f.write(f"{type(e).__name__}: {e}\n{traceback.format_exc()}")
 
 
+def _bucket_worker(rank, world, port, result_dir):
+    try:
+        os.environ["MASTER_ADDR"] = "127.0.0.1"
+        os.environ["MASTER_PORT"] = str(port)
+        from datetime import timedelta
+        dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=20))
+        calls = []
+        real = dist.all_reduce
+
+        def counting(t, *a, **k):
+            calls.append(t.numel())
+            return real(t, *a, **k)
+
+        dist.all_reduce = counting
+        g = torch.Generator().manual_seed(rank)
+        ts = [torch.randn(5, 3, generator=g, dtype=torch.float64), None,
+              torch.randn(5, 4, generator=g, dtype=torch.float64), torch.randn(5, generator=g, dtype=torch.float64)]
+        D.allreduce_gradients(ts)
+        dist.all_reduce = real
+        if rank == 0:
+            torch.save({"calls": calls, "ts": [t for t in ts if t is not None]}, os.path.join(result_dir, "b0.pt"))
+        dist.barrier()
+        dist.destroy_process_group()
+    except Exception as e:
+        with open(os.path.join(result_dir, f"err{rank}.txt"), "w") as f:
+            f.write(f"{type(e).__name__}: {e}\n{traceback.format_exc()}")
+
+
+def test_one_bucketed_allreduce(tmp_path):
+    port = _free_port()
+    mp.start_processes(_bucket_worker, args=(2, port, str(tmp_path)), nprocs=2, join=True, start_method="spawn")
+    assert not list(tmp_path.glob("err*.txt")), [p.read_text() for p in tmp_path.glob("err*.txt")]
+    res = torch.load(tmp_path / "b0.pt")
+    assert res["calls"] == [15 + 20 + 5]  # one collective over the packed bucket
+    want = []
+    for r in range(2):
+        g = torch.Generator().manual_seed(r)
+        want.append([torch.randn(5, 3, generator=g, dtype=torch.float64),
+                     torch.randn(5, 4, generator=g, dtype=torch.float64), torch.randn(5, generator=g, dtype=torch.float64)])
+    for got, a, b in zip(res["ts"], want[0], want[1]):
+        torch.testing.assert_close(got, a + b)
+
+
 def test_view_shard_round_robin():
     v = list(range(7))
     shards = [D.view_shard(v, r, 3) for r in range(3)]

@@ -63,13 +63,15 @@ def test_small_uniform_sh0():
     _assert_parity(fwd, tri, _oracle(sc, ro, rd))
 
 
+@pytest.mark.parametrize("sh_degree", [None, 3])
 @pytest.mark.parametrize("traversal", [0, 1])
 @pytest.mark.parametrize("kbuf,block", [(8, 64), (16, 128), (32, 256)])
-def test_sh3_scene_all_launch_shapes(kbuf, block, traversal):
+def test_sh3_scene_all_launch_shapes(kbuf, block, traversal, sh_degree):
     sc = S.uniform_scene(3000, 3, seed=7)
     ro, rd = S.look_at_rays(S.Camera(S.sphere_point(3.0, 7), 40, 30, 60.0))
-    _, fwd, tri = _gpu_trace(sc, ro, rd, tune=T.Tune(kbuf=kbuf, block=block, traversal=traversal))
-    _assert_parity(fwd, tri, _oracle(sc, ro, rd))
+    _, fwd, tri = _gpu_trace(sc, ro, rd, sh_degree=sh_degree,
+                             tune=T.Tune(kbuf=kbuf, block=block, traversal=traversal))
+    _assert_parity(fwd, tri, _oracle(sc, ro, rd, sh_degree=sh_degree))
 
 
 def test_clustered_scene_subset():
