@@ -189,23 +189,26 @@ def cpu_baseline(sc, ro, rd, threads, target_s=10.0, n_rays=0):
 def small_cpu_baselines(threads):
     """The CPU paths on the small workload (1,000 uniform ellipsoids, SH0, one 64x64 view):
     the reference's quadrature oracle as restated in numpy (2^16 samples per ray; a seeded
-    2-ray sample, single-threaded) and the exact CPU tracer's full forward (all threads)."""
+    sample of one ray per host thread, all threads) and the exact CPU tracer's full forward
+    (all threads)."""
     from ever_b200 import synthetic as S
     from oracle import oracle as O
     from oracle import quad_np as Q
     sc, cams = S.workload_small()
     ro, rd = S.look_at_rays(cams[0])
-    idx = np.sort(np.random.default_rng(0).choice(ro.shape[0], 2, replace=False))
+    nq = max(2, threads)
+    idx = np.sort(np.random.default_rng(0).choice(ro.shape[0], nq, replace=False))
     t0 = time.perf_counter()
-    Q.trace_rays(sc.mean, sc.scale, sc.quat, sc.density.reshape(-1), sc.features.reshape(-1, 3), ro[idx], rd[idx])
+    Q.trace_rays(sc.mean, sc.scale, sc.quat, sc.density.reshape(-1), sc.features.reshape(-1, 3), ro[idx], rd[idx],
+                 nthreads=threads)
     tq = time.perf_counter() - t0
     s = O.Scene(sc.mean, sc.scale, sc.quat, sc.density.reshape(-1), sc.features)
     O.trace(s, ro, rd, 0.0, 1000.0, 500, nthreads=threads)
     t0 = time.perf_counter()
     O.trace(s, ro, rd, 0.0, 1000.0, 500, nthreads=threads)
     te = time.perf_counter() - t0
-    return {"quad_np": {"rays_per_s": 2 / tq, "cores": 1, "sample": "2 seeded rays of the 64x64 view",
-                        "full_view_s_extrapolated": ro.shape[0] * tq / 2},
+    return {"quad_np": {"rays_per_s": nq / tq, "cores": threads, "sample": f"{nq} seeded rays of the 64x64 view",
+                        "full_view_s_extrapolated": ro.shape[0] * tq / nq},
             "exact_cpu_forward": {"rays_per_s": ro.shape[0] / te, "cores": threads, "sample": "the full 64x64 view",
                                   "ms": te * 1e3}}
 
@@ -230,7 +233,8 @@ def run_reference(args):
         "data": "synthetic (seeded clustered scene; no trained scenes ship with the reference)",
         "config": {"workload": workload_name(args), "sample": f"{n} seeded rays of the view per step"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{n} rays of the {args.width}x{args.height} view per step, all ellipsoids"},
+                         "sample": f"{n} rays of the {args.width}x{args.height} view per step, all ellipsoids",
+                         "note": "brute force, O(N) ellipsoid tests per ray, no BVH"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "reference OptiX/Slang tracer unavailable on this box (no OptiX SDK, slangc, glm, CGAL, absl); "
                 "timed: the CPU restatement of its trace path (oracle/ever_oracle.cpp)",
@@ -724,7 +728,9 @@ def main():
         threads = os.cpu_count() or 1
         v, dt, n = cpu_baseline(sc, ro, rd, threads, target_s=10.0, n_rays=args.cpu_sample)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                                "sample": f"{n} seeded rays of the view, forward + FP64 backward, {dt:.1f} s"}
+                                "sample": f"{n} seeded rays of the view, forward + FP64 backward, {dt:.1f} s",
+                                "note": "the oracle: exact events by brute force, O(N) ellipsoid tests per ray, "
+                                        "no BVH; a correctness tool, not a tuned CPU tracer"}
         line["cpu_baselines_small"] = small_cpu_baselines(threads)
     if rank == 0 and world == 1 and not args.no_batched:
         line["camera"] = leg_camera(dev, args)

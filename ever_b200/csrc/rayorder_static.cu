@@ -15,9 +15,11 @@
 // the GPU (different streams, or work queued from different host threads) race on the
 // array, so a caller must order them, e.g. by using one stream.
 //
-// Set-up: the device address of the array is looked up once per device, by the first
-// call made while that device is current, through cudaGetSymbolAddress. Make that first
-// call before any stream capture on the device.
+// Set-up: the device address of the array is looked up through cudaGetSymbolAddress on
+// every call whose stream is not capturing, and kept per device for the calls made during
+// a stream capture (where that lookup could load the module and break the capture). So
+// make one call on each device before capturing one; after cudaDeviceReset the next
+// uncaptured call looks the address up again.
 #include <mutex>
 
 #include "common.cuh"
@@ -47,22 +49,28 @@ extern "C" int ever_ray_order_static(const float* rayo, const float* rayd, int64
   if (num_rays < 0 || num_rays > kStaticOrderMaxRays)
     return set_last_error(EVER_ERR_INVALID,
                      "ever_ray_order_static: num_rays out of range [0, 2097152]; use ever_ray_order with a workspace");
-  if (num_rays > 0 && (!rayo || !rayd || !ray_order)) return set_last_error(EVER_ERR_INVALID, "ever_ray_order_static: null pointer");
   if (ever::ray_order_workspace(num_rays) > kStaticOrderBytes)
     return set_last_error(EVER_ERR_INVALID, "ever_ray_order_static: scratch layout larger than the static array");
+  if (num_rays > 0 && (!rayo || !rayd || !ray_order)) return set_last_error(EVER_ERR_INVALID, "ever_ray_order_static: null pointer");
   if (num_rays == 0) return EVER_OK;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return set_last_error(EVER_ERR_CUDA, cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) return set_last_error(EVER_ERR_INVALID, "ever_ray_order_static: device index too large");
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(static_cast<cudaStream_t>(stream), &cap);
+  if (e != cudaSuccess) return set_last_error(EVER_ERR_CUDA, cudaGetErrorString(e));
   void* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_scratch_ptr[dev]) {
+    if (cap == cudaStreamCaptureStatusNone) {
       void* p = nullptr;
       e = cudaGetSymbolAddress(&p, g_order_scratch);
       if (e != cudaSuccess) return set_last_error(EVER_ERR_CUDA, cudaGetErrorString(e));
       g_scratch_ptr[dev] = p;
+    } else if (!g_scratch_ptr[dev]) {
+      return set_last_error(EVER_ERR_INVALID,
+                            "ever_ray_order_static: first call on this device made during a stream capture");
     }
     scratch = g_scratch_ptr[dev];
   }

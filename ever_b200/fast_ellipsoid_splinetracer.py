@@ -25,6 +25,10 @@ gradients of the image it returned. Opt in to view-dependent colour with sh_degr
 (1..3, needs (d+1)^2 <= K): SH of degree d evaluated along the raw ray direction rayd in
 both passes.
 
+Status: the kernels never trap; overflows of fixed-size device structures raise flags in
+a status word, returned as extras["status"] with return_extras=True (see the EVER_STATUS_*
+flags in include/ever_b200.h).
+
 Launch order: by default the rays are first sorted into a coherent order on the device
 (ray_order="auto", see ever_ray_order in include/ever_b200.h) so that each warp's packet
 covers a compact patch of directions; pass ray_order=None for the given order or an
@@ -107,6 +111,11 @@ class SplineTracer(Function):
                 touch_count=fwd.touch_count,
                 distortion_loss=out[:, 4],
                 saved=saved,
+                # (1,) int32 OR of the EVER_STATUS_* flags the kernels raised (0: clean). Not a
+                # reference key: 1 = a traversal stack overflowed (a BVH subtree was skipped),
+                # 2 = the event log was too short, 4 = more than 16 ellipsoids contain a ray
+                # start (still summed). Read it without a host sync until you need it.
+                status=fwd.status,
             )
         return out
 

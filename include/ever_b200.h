@@ -44,7 +44,7 @@ typedef struct EverScene {
   int32_t sh_coeffs;  /* K: SH coefficients stored per ellipsoid (feature stride) */
   int32_t num_nodes;  /* internal BVH nodes: max(N-1, 1), 0 if N == 0 */
   void* nodes;        /* num_nodes x 64 B: child boxes + child links */
-  void* records;      /* N x 64 B: 3x3 local-frame matrix, mean, density, index */
+  void* records;      /* N x 64 B: 3x3 local-frame matrix, mean, density, DC colour */
   float* features;    /* N rows of 3K floats padded to a multiple of 4, Morton order */
   int32_t* order;     /* N: Morton position -> original ellipsoid index */
   void* scratch;      /* build-time scratch inside the workspace */
@@ -213,10 +213,11 @@ int ever_ray_order(const float* rayo, const float* rayd, int64_t num_rays, void*
  * waits for the whole device), or a binding from another runtime that cannot hand this
  * library a workspace. Its scratch is a static device array of about 33 MB built into the
  * library, held by every GPU that loads it until exit; num_rays must be <= 2,097,152 (one
- * 1920x1080 view), larger counts return EVER_ERR_INVALID. The first call on a device looks
- * the array's address up (make it before any stream capture); calls that overlap on the
- * GPU share the array and race, so order them (e.g. one stream). Same output as
- * ever_ray_order. */
+ * 1920x1080 view), larger counts return EVER_ERR_INVALID. Each call outside a stream
+ * capture looks the array's address up (cudaGetSymbolAddress) and keeps it for calls made
+ * during a capture, so make one call on a device before capturing there; calls that
+ * overlap on the GPU share the array and race, so order them (e.g. one stream). Same
+ * output as ever_ray_order. */
 int ever_ray_order_static(const float* rayo, const float* rayd, int64_t num_rays, int32_t* ray_order,
                           void* stream);
 

@@ -93,8 +93,16 @@ def trace_ray(mean, scale, quat, density, features, rayo, rayd, tmin=0.0, tmax=1
 
 
 def trace_rays(mean, scale, quat, density, features, rayo, rayd, tmin=0.0, tmax=1000.0,
-               num_quad=2 ** 16):
+               num_quad=2 ** 16, nthreads=1):
+    """(R, 5) for R rays; nthreads > 1 traces rays on that many threads (numpy releases the
+    GIL inside its array loops, which hold nearly all of the work)."""
     rayo = np.asarray(rayo, np.float64).reshape(-1, 3)
     rayd = np.asarray(rayd, np.float64).reshape(-1, 3)
-    return np.stack([trace_ray(mean, scale, quat, density, features, rayo[i], rayd[i], tmin, tmax, num_quad)
-                     for i in range(rayo.shape[0])])
+    one = lambda i: trace_ray(mean, scale, quat, density, features, rayo[i], rayd[i], tmin, tmax, num_quad)
+    if nthreads <= 1 or rayo.shape[0] <= 1:
+        rows = [one(i) for i in range(rayo.shape[0])]
+    else:
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(max_workers=int(nthreads)) as ex:
+            rows = list(ex.map(one, range(rayo.shape[0])))
+    return np.stack(rows) if rows else np.zeros((0, 5))

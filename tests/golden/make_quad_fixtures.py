@@ -1,7 +1,10 @@
 """Generates tests/golden/quad_*.npz by running the reference's own quadrature oracle.
 
-Runs only where the reference tree is mounted (it reads /root/reference); the GPU
-box and the test suite only read the committed .npz files.
+Runs only where the reference tree is available: pass its root as the first argument
+or in the EVER_REFERENCE environment variable. The GPU box and the test suite only read
+the committed .npz files.
+
+    python tests/golden/make_quad_fixtures.py <path to the N-Demir/ever tree>
 
 The reference oracle (splinetracers/quad.py, jaxutil/quadrature.py,
 jaxutil/safe_math.py, utils/math_util.py) is imported unmodified from the reference
@@ -29,7 +32,7 @@ import types
 
 import numpy as np
 
-REF = "/root/reference"
+REF = None  # the reference tree's root, set by main() from argv[1] or EVER_REFERENCE
 OUT_DIR = os.path.dirname(os.path.abspath(__file__))
 
 _JAX_STANDIN = r'''
@@ -141,7 +144,11 @@ def _cases(rng):
 
 
 def main():
+    global REF
     import torch
+    REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("EVER_REFERENCE")
+    if not REF or not os.path.isdir(os.path.join(REF, "splinetracers")):
+        sys.exit("usage: make_quad_fixtures.py <reference tree root> (or set EVER_REFERENCE)")
     with tempfile.TemporaryDirectory() as tmp:
         _install_standins(tmp)
         quad = _load_reference_quad()

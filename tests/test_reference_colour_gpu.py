@@ -35,6 +35,7 @@ def _run(sc, ro, rd, dout, **kw):
     out, extras = trace_rays(t["mean"], t["scale"], t["quat"], t["density"], t["features"], rayo, rayd,
                              return_extras=True, **kw)
     (out * torch.tensor(dout, dtype=torch.float32, device=dev)).sum().backward()
+    assert int(extras["status"].item()) == 0
     g = {k: v.grad.cpu().double().numpy() for k, v in t.items()}
     g["rayo"], g["rayd"] = rayo.grad.cpu().double().numpy(), rayd.grad.cpu().double().numpy()
     R = ro.shape[0]
@@ -80,7 +81,7 @@ def test_default_is_reference_dc_colour_at_k16():
     assert np.abs(g["features"][:, 0, :]).max() > 0.0
     # the image is the K=1 trace of the DC coefficients, bit for bit
     dc = S.SceneArrays(sc.mean, sc.scale, sc.quat, sc.density, np.ascontiguousarray(sc.features[:, :1]))
-    out1, _, _, g1 = _run(dc, ro, rd, dout)
+    out1, _, _, _ = _run(dc, ro, rd, dout)
     assert np.array_equal(out, out1)
     # and it differs from view-dependent SH: the default is not sh_degree=3
     out3, _, _, _ = _run(sc, ro, rd, dout, sh_degree=3)

@@ -28,6 +28,9 @@ def test_static_ray_order_rejects_too_many_rays():
     assert rc == 1
     assert b"out of range" in lib.ever_last_error()
     assert lib.ever_ray_order_static(None, None, 0, None, None) == 0
+    # exactly the maximum passes the scratch-layout check (it fails later, on the null pointers)
+    assert lib.ever_ray_order_static(None, None, MAX_RAYS, None, None) == 1
+    assert b"null pointer" in lib.ever_last_error()
 
 
 @pytest.mark.gpu
@@ -37,7 +40,8 @@ def test_static_ray_order_matches_workspace_version():
     lib = N.load()
     dev = torch.device("cuda:0")
     # consecutive calls of different sizes: the static array keeps the previous call's contents
-    for W, H, seed in [(640, 480, 1), (1920, 1080, 2), (320, 240, 3)]:
+    # the last size is exactly the documented maximum: keys, values and histogram fill the array
+    for W, H, seed in [(640, 480, 1), (1920, 1080, 2), (320, 240, 3), (2048, 1024, 4)]:
         ro, rd = S.look_at_rays(S.Camera(S.sphere_point(4.0, seed), W, H, 50.0))
         rayo = torch.tensor(ro, device=dev)
         rayd = torch.tensor(rd, device=dev)
