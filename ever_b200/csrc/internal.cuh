@@ -70,6 +70,7 @@ struct FwdParams {
   int max_iters;
   const int32_t* ray_order;
   EverForwardOut out;
+  int frustum;  // packet kernels: frustum phase before the rounds (set from the tune)
 };
 
 cudaError_t launch_forward(const FwdParams& P, int deg, const EverTune& tune, cudaStream_t st);
@@ -141,6 +142,7 @@ struct BatchFwdParams {
   EverForwardOut out;  // ray-indexed outputs; event_log columns are slots (stride num_slots)
   unsigned int* work_counter;
   int grid;            // persistent blocks
+  int frustum;         // frustum phase before the rounds (set from the tune)
 };
 
 cudaError_t launch_forward_batched(const BatchFwdParams& P, int deg, const EverTune& tune, cudaStream_t st);

@@ -119,8 +119,16 @@ cudaError_t regroup_compact(const uint32_t* mask, const uint32_t* n_dev, int64_t
   return cudaGetLastError();
 }
 
-cudaError_t launch_forward_regrouped(const FwdParams& P, const RegroupScratch& W, const CameraParams* cam,
+// traversal 0: warp packets with the frustum phase; 2: warp packets, rounds only
+FwdParams with_mode(const FwdParams& P0, const EverTune& tune) {
+  FwdParams P = P0;
+  P.frustum = tune.traversal == 0 ? 1 : 0;
+  return P;
+}
+
+cudaError_t launch_forward_regrouped(const FwdParams& P0, const RegroupScratch& W, const CameraParams* cam,
                                      const float* jitter, int deg, const EverTune& tune, cudaStream_t st) {
+  const FwdParams P = with_mode(P0, tune);
   if (P.R == 0) return cudaSuccess;
   const int block = tune.block > 0 ? tune.block : 128;
   // splitting pays only while the next pass still fills the GPU several times over: four
@@ -132,7 +140,7 @@ cudaError_t launch_forward_regrouped(const FwdParams& P, const RegroupScratch& W
   const int64_t n = cam ? camera_slots(*cam) : P.R;
   if (n < V.split_min) {  // one pass would run every round: the single packet kernel does the same
     EverTune t = tune;
-    t.traversal = 0;
+    if (t.traversal == 1) t.traversal = 0;
     return cam ? launch_forward_camera(P, *cam, jitter, deg, t, st) : launch_forward(P, deg, t, st);
   }
   switch (tune.kbuf) {
@@ -142,7 +150,9 @@ cudaError_t launch_forward_regrouped(const FwdParams& P, const RegroupScratch& W
   }
 }
 
-cudaError_t launch_forward_batched(const BatchFwdParams& P, int deg, const EverTune& tune, cudaStream_t st) {
+cudaError_t launch_forward_batched(const BatchFwdParams& P0, int deg, const EverTune& tune, cudaStream_t st) {
+  BatchFwdParams P = P0;
+  P.frustum = tune.traversal == 2 ? 0 : 1;
   if (P.num_slots == 0) return cudaSuccess;
   const int block = tune.block > 0 ? tune.block : 128;
   switch (tune.kbuf) {
@@ -152,7 +162,8 @@ cudaError_t launch_forward_batched(const BatchFwdParams& P, int deg, const EverT
   }
 }
 
-cudaError_t launch_forward(const FwdParams& P, int deg, const EverTune& tune, cudaStream_t st) {
+cudaError_t launch_forward(const FwdParams& P0, int deg, const EverTune& tune, cudaStream_t st) {
+  const FwdParams P = with_mode(P0, tune);
   if (P.R == 0) return cudaSuccess;
   const int block = tune.block > 0 ? tune.block : 128;
   switch (tune.kbuf) {
@@ -162,8 +173,9 @@ cudaError_t launch_forward(const FwdParams& P, int deg, const EverTune& tune, cu
   }
 }
 
-cudaError_t launch_forward_camera(const FwdParams& P, const CameraParams& cam, const float* jitter, int deg,
+cudaError_t launch_forward_camera(const FwdParams& P0, const CameraParams& cam, const float* jitter, int deg,
                                   const EverTune& tune, cudaStream_t st) {
+  const FwdParams P = with_mode(P0, tune);
   if (int64_t(cam.width) * cam.height == 0) return cudaSuccess;
   const int block = tune.block > 0 ? tune.block : 128;
   switch (tune.kbuf) {

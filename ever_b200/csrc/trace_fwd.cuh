@@ -294,14 +294,53 @@ struct TraceCtx {
   int max_iters;
   int64_t log_stride;  // event-log row length (slots)
   EverForwardOut out;
+  bool frustum;        // packet kernels: run the frustum phase before the rounds
 };
+
+// One event of a ray's sorted sequence, integrated under the reference's round rules
+// (shaders.slang:197-227): an event tied with the 16th event of a reference round is
+// dropped, an exit beyond tmax counts only inside the round that consumed its entry, a
+// t > 1e9 sentinel ends the ray. Returns true once the ray is finished.
+template <int DEG>
+__device__ __forceinline__ bool consume_event(const SceneRef& sc, const TraceCtx& C, const Ray& ray, const float* B,
+                                              int bs, int64_t slot, uint64_t k, State& s, float4& last_dirac,
+                                              int& iters, float& s16, int& cnt16, uint32_t& status) {
+  const float t = key_t(k);
+  const int j = key_pos(k);
+  const int ex = key_exit(k);
+  if (!(t > s16)) return false;  // tied with the 16th event of a reference round: dropped
+  if (t > kSentinel) return true;
+  const float4 r3 = __ldg(&sc.recs[j].r3);
+  if (ex && t > C.tmax) {
+    HitT H;
+    intersect(load_record(sc.recs, j), ray, H);
+    if (!(H.t0 > s16 && H.t0 <= C.tmax)) return false;
+  }
+  const float3 c = DEG == 0 ? dc_colour(r3) : sh_colour<DEG>(sc.features + int64_t(j) * feat_stride(sc.K), B, bs);
+  const float dh = ex ? -r3.x : r3.x;
+  const float4 dirac = make_float4(dh, dh * c.x, dh * c.y, dh * c.z);
+  update(s, t, dirac);
+  last_dirac = dirac;
+  if (C.out.event_log) {
+    if (iters < C.out.log_cap)
+      C.out.event_log[int64_t(iters) * C.log_stride + slot] = 2 * j + (ex ? 0 : 1);
+    else
+      status |= EVER_STATUS_LOG_OVERFLOW;
+  }
+  if (C.out.touch_count) atomicAdd(C.out.touch_count + __ldg(sc.order + j), 1);
+  ++iters;
+  if (++cnt16 == kRefRound) {
+    s16 = t;
+    cnt16 = 0;
+  }
+  return !(s.logT < kLogCutoff && iters < C.max_iters);
+}
 
 // Integrates the gathered events in order. Returns true once the ray is finished.
 template <int KBUF, int DEG>
 __device__ __forceinline__ bool consume(const SceneRef& sc, const TraceCtx& C, const Ray& ray, const float* B,
                                         int bs, int64_t slot, uint64_t (&buf)[KBUF], State& s, float4& last_dirac,
                                         int& iters, float& s16, int& cnt16, uint64_t& lower, uint32_t& status) {
-  const int fst = feat_stride(sc.K);
   const uint64_t last = buf[KBUF - 1];
   bool done = false;
   for (int n = 0; n < KBUF && !done; ++n) {
@@ -310,35 +349,7 @@ __device__ __forceinline__ bool consume(const SceneRef& sc, const TraceCtx& C, c
     for (int i = 0; i < KBUF - 1; ++i) buf[i] = buf[i + 1];
     buf[KBUF - 1] = kEmptyKey;
     if (k == kEmptyKey) return true;  // nothing left beyond the last gathered event
-    const float t = key_t(k);
-    const int j = key_pos(k);
-    const int ex = key_exit(k);
-    if (!(t > s16)) continue;  // tied with the 16th event of a reference round: dropped
-    if (t > kSentinel) return true;
-    const float4 r3 = __ldg(&sc.recs[j].r3);
-    if (ex && t > C.tmax) {
-      HitT H;
-      intersect(load_record(sc.recs, j), ray, H);
-      if (!(H.t0 > s16 && H.t0 <= C.tmax)) continue;
-    }
-    const float3 c = DEG == 0 ? dc_colour(r3) : sh_colour<DEG>(sc.features + int64_t(j) * fst, B, bs);
-    const float dh = ex ? -r3.x : r3.x;
-    const float4 dirac = make_float4(dh, dh * c.x, dh * c.y, dh * c.z);
-    update(s, t, dirac);
-    last_dirac = dirac;
-    if (C.out.event_log) {
-      if (iters < C.out.log_cap)
-        C.out.event_log[int64_t(iters) * C.log_stride + slot] = 2 * j + (ex ? 0 : 1);
-      else
-        status |= EVER_STATUS_LOG_OVERFLOW;
-    }
-    if (C.out.touch_count) atomicAdd(C.out.touch_count + __ldg(sc.order + j), 1);
-    ++iters;
-    if (++cnt16 == kRefRound) {
-      s16 = t;
-      cnt16 = 0;
-    }
-    if (!(s.logT < kLogCutoff && iters < C.max_iters)) done = true;
+    done = consume_event<DEG>(sc, C, ray, B, bs, slot, k, s, last_dirac, iters, s16, cnt16, status);
   }
   if (done || last == kEmptyKey) return true;
   lower = last;
@@ -413,7 +424,7 @@ __global__ void __launch_bounds__(256) k_trace_fwd_ray(const FwdParams P) {
   if (gi >= P.R) return;
   const int64_t r = P.ray_order ? int64_t(P.ray_order[gi]) : gi;
   const SceneRef sc = scene_of(P);
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out};
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out, P.frustum != 0};
   const Ray ray = load_ray(P.rayo, P.rayd, r, P.tmin);
   const RaySlab sl = make_slab(ray);
   float B[16];
@@ -506,6 +517,232 @@ __device__ __forceinline__ bool run_rounds(const SceneRef& sc, const TraceCtx& C
   return act;
 }
 
+// ---- packet frustum phase ----
+// The warp bounds its active rays by intervals (origins, directions, inverse directions),
+// walks the BVH breadth first with one node per lane, keeping every child box some packet
+// ray can meet (a conservative interval slab test), and lists the leaves sorted by the
+// earliest t at which any packet ray can enter them. Every lane then takes the leaves in
+// that order: the leaf's events on its own ray go into its sorted buffer, and before the
+// next leaf, whose events all lie at or beyond that leaf's entry bound T, the events
+// below T are final and are integrated in order. So each ray integrates exactly its
+// sorted event sequence, as the rounds do, with one walk per packet instead of one per
+// round, and the box tests spread over the lanes instead of repeating for every ray.
+// A lane whose buffer would overflow, and every lane of a packet whose breadth-first
+// lists overflow shared memory, stops after its last integrated event; the rounds then
+// continue it from there (lower = that event's key), so the results do not depend on it.
+constexpr int kFrontierCap = 384;  // nodes per breadth-first level
+constexpr int kCandCap = 512;      // leaves per packet (a power of two: the sort's width)
+// Shared ints per warp: the traversal stack, two frontier levels, the leaf keys (64-bit).
+constexpr int kWarpInts = kStackDepth + 2 * kFrontierCap + 2 * kCandCap;
+
+__device__ __forceinline__ uint32_t ordered_bits(float f) {
+  const uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float from_ordered(uint32_t u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+__device__ __forceinline__ float warp_min(float v) { return from_ordered(__reduce_min_sync(kFull, ordered_bits(v))); }
+__device__ __forceinline__ float warp_max(float v) { return from_ordered(__reduce_max_sync(kFull, ordered_bits(v))); }
+
+struct PacketBounds {
+  float omin[3], omax[3];  // origins
+  float imin[3], imax[3];  // inverse directions (as the per-ray slab test takes them)
+  float dmin[3], dmax[3];  // unit directions
+  unsigned free_axes;      // axes whose direction changes sign within the packet
+};
+
+// Interval bounds over the lanes with `part` (all lanes take part in the reductions).
+__device__ __forceinline__ PacketBounds packet_bounds(const Ray& ray, const RaySlab& sl, bool part) {
+  PacketBounds P;
+  const float o[3] = {ray.o.x, ray.o.y, ray.o.z}, d[3] = {ray.d.x, ray.d.y, ray.d.z};
+  const float iv[3] = {sl.invd.x, sl.invd.y, sl.invd.z};
+  P.free_axes = 0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    P.omin[a] = warp_min(part ? o[a] : INFINITY);
+    P.omax[a] = warp_max(part ? o[a] : -INFINITY);
+    P.imin[a] = warp_min(part ? iv[a] : INFINITY);
+    P.imax[a] = warp_max(part ? iv[a] : -INFINITY);
+    P.dmin[a] = warp_min(part ? d[a] : INFINITY);
+    P.dmax[a] = warp_max(part ? d[a] : -INFINITY);
+    if (P.imin[a] < 0.f && P.imax[a] > 0.f) P.free_axes |= 1u << a;
+  }
+  return P;
+}
+
+__device__ __forceinline__ float min4(float a, float b, float c, float d) { return fminf(fminf(a, b), fminf(c, d)); }
+__device__ __forceinline__ float max4(float a, float b, float c, float d) { return fmaxf(fmaxf(a, b), fmaxf(c, d)); }
+
+// A lower bound of the t at which any packet ray enters the box within [0, cap], or +inf
+// when no packet ray can meet it there. Interval products bound every ray's plane
+// distances; the float rounding of the bound (a few ulps) is covered by widening it by a
+// relative 1e-6. Axes whose direction changes sign bound no t: there the positions the
+// packet reaches over the t range of the other axes must overlap the box.
+__device__ __forceinline__ float packet_entry(const PacketBounds& P, float lx, float ly, float lz, float hx, float hy,
+                                              float hz, float cap) {
+  const float lo[3] = {lx, ly, lz}, hi[3] = {hx, hy, hz};
+  float tn = 0.f, tf = cap;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (P.free_axes >> a & 1u) continue;
+    const float d0 = lo[a] - P.omax[a], d1 = lo[a] - P.omin[a];
+    const float e0 = hi[a] - P.omax[a], e1 = hi[a] - P.omin[a];
+    const float p0 = d0 * P.imin[a], p1 = d0 * P.imax[a], p2 = d1 * P.imin[a], p3 = d1 * P.imax[a];
+    const float q0 = e0 * P.imin[a], q1 = e0 * P.imax[a], q2 = e1 * P.imin[a], q3 = e1 * P.imax[a];
+    tn = fmaxf(tn, fminf(min4(p0, p1, p2, p3), min4(q0, q1, q2, q3)));
+    tf = fminf(tf, fmaxf(max4(p0, p1, p2, p3), max4(q0, q1, q2, q3)));
+  }
+  tn = tn - 1e-6f * fabsf(tn);
+  tf = tf + 1e-6f * fabsf(tf);
+  if (!(tn <= tf)) return INFINITY;
+  if (P.free_axes) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      if (!(P.free_axes >> a & 1u)) continue;
+      const float xl = P.omin[a] + min4(tn * P.dmin[a], tn * P.dmax[a], tf * P.dmin[a], tf * P.dmax[a]);
+      const float xh = P.omax[a] + max4(tn * P.dmin[a], tn * P.dmax[a], tf * P.dmin[a], tf * P.dmax[a]);
+      const float tol = 1e-6f * (fabsf(xl) + fabsf(xh) + fabsf(tf));
+      if (xh + tol < lo[a] || xl - tol > hi[a]) return INFINITY;
+    }
+  }
+  return fmaxf(tn, 0.f);
+}
+
+// Breadth-first walk: the leaf keys (entry bound bits << 32 | position) of every leaf the
+// packet can meet, into cand[0, n). Returns n, or -1 when a level or the leaf list does
+// not fit its shared-memory capacity.
+__device__ __forceinline__ int packet_leaves(const Node* __restrict__ nodes, const PacketBounds& P, float cap,
+                                             int* front, uint64_t* cand, int lane) {
+  int* cur = front;
+  int* nxt = front + kFrontierCap;
+  if (lane == 0) cur[0] = 0;
+  __syncwarp();
+  int nf = 1, nc = 0;
+  const unsigned below = (1u << lane) - 1u;
+  for (int level = 0; nf > 0; ++level) {
+    if (level >= 4 * kStackDepth) return -1;  // deeper than any tree the build makes
+    int nn = 0;
+    for (int base = 0; base < nf; base += 32) {
+      const int i = base + lane;
+      float te0 = INFINITY, te1 = INFINITY;
+      int c0 = 0, c1 = 0;
+      if (i < nf) {
+        const Node nd = load_node(nodes, cur[i]);
+        te0 = packet_entry(P, nd.a.x, nd.a.y, nd.a.z, nd.a.w, nd.b.x, nd.b.y, cap);
+        te1 = packet_entry(P, nd.b.z, nd.b.w, nd.c.x, nd.c.y, nd.c.z, nd.c.w, cap);
+        c0 = nd.d.x;
+        c1 = nd.d.y;
+      }
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const float te = k ? te1 : te0;
+        const int c = k ? c1 : c0;
+        const bool hit = te != INFINITY;
+        const unsigned mi = __ballot_sync(kFull, hit && c >= 0);
+        const unsigned ml = __ballot_sync(kFull, hit && c < 0);
+        if (hit && c >= 0) {
+          const int q = nn + __popc(mi & below);
+          if (q < kFrontierCap) nxt[q] = c;
+        }
+        if (hit && c < 0) {
+          const int q = nc + __popc(ml & below);
+          if (q < kCandCap) cand[q] = (uint64_t(__float_as_uint(te)) << 32) | uint32_t(~c);
+        }
+        nn += __popc(mi);
+        nc += __popc(ml);
+      }
+    }
+    __syncwarp();
+    if (nn > kFrontierCap || nc > kCandCap) return -1;
+    int* t = cur;
+    cur = nxt;
+    nxt = t;
+    nf = nn;
+  }
+  return nc;
+}
+
+// Ascending bitonic sort of cand[0, n) in shared memory by the warp (n <= kCandCap).
+__device__ __forceinline__ void sort_keys(uint64_t* cand, int n, int lane) {
+  int w = 32;
+  while (w < n) w <<= 1;
+  for (int i = n + lane; i < w; i += 32) cand[i] = kEmptyKey;
+  __syncwarp();
+  for (int k = 2; k <= w; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = lane; i < w; i += 32) {
+        const int l = i ^ j;
+        if (l > i) {
+          const uint64_t a = cand[i], b = cand[l];
+          if ((a > b) == ((i & k) == 0)) {
+            cand[i] = b;
+            cand[l] = a;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// The frustum phase of a warp's packet. Returns whether this lane's ray still needs rounds
+// (L then holds its state after its last integrated event, L.lower that event's key).
+template <int KBUF, int DEG>
+__device__ bool frustum_phase(const SceneRef& sc, const TraceCtx& C, const Ray& ray, const float* B, int bs,
+                              int64_t slot, int* wsm, int lane, bool act, RayLoop& L) {
+  if (!__any_sync(kFull, act)) return act;
+  const RaySlab sl = make_slab(ray);
+  const float cap = fminf(C.tmax, kSentinel);
+  const PacketBounds P = packet_bounds(ray, sl, act);
+  int* front = wsm + kStackDepth;
+  uint64_t* cand = reinterpret_cast<uint64_t*>(front + 2 * kFrontierCap);
+  const int nc = packet_leaves(sc.nodes, P, cap, front, cand, lane);
+  if (nc < 0) return act;  // lists too long for shared memory: the rounds trace the packet
+  sort_keys(cand, nc, lane);
+  uint64_t buf[KBUF];
+#pragma unroll
+  for (int i = 0; i < KBUF; ++i) buf[i] = kEmptyKey;
+  bool live = act;  // still integrating in this phase
+  for (int ci = 0;; ++ci) {
+    const uint64_t ck = ci < nc ? cand[ci] : kEmptyKey;
+    const float T = ci < nc ? key_t(ck) : INFINITY;
+    // events below T are final: no leaf still to come has an event before T
+    while (live && buf[0] != kEmptyKey && key_t(buf[0]) < T) {
+      const uint64_t k = buf[0];
+#pragma unroll
+      for (int i = 0; i < KBUF - 1; ++i) buf[i] = buf[i + 1];
+      buf[KBUF - 1] = kEmptyKey;
+      L.lower = k;
+      if (consume_event<DEG>(sc, C, ray, B, bs, slot, k, L.s, L.last_dirac, L.iters, L.s16, L.cnt16, L.status)) {
+        live = false;
+        act = false;  // finished
+      }
+    }
+    if (ci >= nc) break;
+    if (!__any_sync(kFull, live)) break;
+    if (live) {
+      const int j = int(uint32_t(ck));
+      const Record R = load_record(sc.recs, j);
+      HitT H;
+      if (intersect(R, ray, H)) {
+        const bool in0 = H.t0 > L.s16 && H.t0 <= C.tmax;
+        const bool in1 = H.t1 > L.s16 && (H.t1 <= C.tmax || in0);
+        // a full buffer cannot take another event: stop here, the rounds continue the ray
+        if ((in0 || in1) && buf[KBUF - (in0 && in1 ? 2 : 1)] != kEmptyKey) {
+          live = false;
+        } else {
+          if (in0) buf_insert(buf, event_key(H.t0, j, 0));
+          if (in1) buf_insert(buf, event_key(H.t1, j, 1));
+        }
+      }
+    }
+  }
+  // all leaves taken and every event integrated: nothing is left on a lane still active
+  if (live) act = false;
+  return act;
+}
+
 // One warp traces one packet of up to 32 rays against one scene (lanes with valid=false
 // only take part in the warp-wide votes).
 template <int KBUF, int DEG>
@@ -513,7 +750,9 @@ __device__ __forceinline__ void trace_packet(const SceneRef& sc, const TraceCtx&
                                              bool valid, int64_t slot, int* wstack, float* B, int bs, int lane) {
   store_basis<DEG>(ray, B, bs);
   RayLoop L = start_ray<DEG>(sc, ray, valid, wstack, B, bs, lane);
-  run_rounds<KBUF, DEG>(sc, C, ray, B, bs, slot, wstack, lane, valid && C.max_iters > 0 && sc.N > 0, L, INT_MAX);
+  bool act = valid && C.max_iters > 0 && sc.N > 0;
+  if (C.frustum) act = frustum_phase<KBUF, DEG>(sc, C, ray, B, bs, slot, wstack, lane, act, L);
+  run_rounds<KBUF, DEG>(sc, C, ray, B, bs, slot, wstack, lane, act, L, INT_MAX);
   if (valid) write_outputs(C.out, r, L.s, L.last_dirac, L.iters, L.status);
   __syncwarp();
 }
@@ -565,12 +804,12 @@ template <int KBUF, int DEG, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value) k_trace_fwd_packet(const FwdParams P) {
   extern __shared__ int smem[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  int* wstack = smem + warp * kStackDepth;
-  float* B = reinterpret_cast<float*>(smem + (blockDim.x / 32) * kStackDepth) + tid;  // B[k * blockDim.x]
+  int* wstack = smem + warp * kWarpInts;  // stack, then the frustum phase's lists
+  float* B = reinterpret_cast<float*>(smem + (blockDim.x / 32) * kWarpInts) + tid;  // B[k * blockDim.x]
   const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;
   const bool valid = gi < P.R;  // every lane stays for the warp-wide ballots
   const int64_t r = valid ? (P.ray_order ? int64_t(P.ray_order[gi]) : gi) : 0;
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out};
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out, P.frustum != 0};
   const Ray ray = load_ray(P.rayo, P.rayd, r, P.tmin);
   trace_packet<KBUF, DEG>(scene_of(P), C, ray, r, valid, gi, wstack, B, blockDim.x, lane);
 }
@@ -597,8 +836,8 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value)
                      uint32_t* __restrict__ mask, int64_t split_min, const PassCamera Q) {
   extern __shared__ int smem[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  int* wstack = smem + warp * kStackDepth;
-  float* B = reinterpret_cast<float*>(smem + (blockDim.x / 32) * kStackDepth) + tid;
+  int* wstack = smem + warp * kWarpInts;  // stack, then the frustum phase's lists
+  float* B = reinterpret_cast<float*>(smem + (blockDim.x / 32) * kWarpInts) + tid;
   const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;  // slot (PASS 0) or list position
   const int64_t slots = CAM ? Q.num_slots : P.R;
   const int64_t n = PASS == 0 ? slots : int64_t(*count);
@@ -614,7 +853,7 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value)
   }
   if (!valid) r = 0;
   const SceneRef sc = scene_of(P);
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, slots, P.out};
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, slots, P.out, P.frustum != 0};
   Ray ray;
   if (CAM) {
     float3 ro, rd;
@@ -629,12 +868,15 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value)
   if (PASS == 0) {
     L = start_ray<DEG>(sc, ray, valid, wstack, B, blockDim.x, lane);
     act = valid && C.max_iters > 0 && sc.N > 0;
+    if (C.frustum) act = frustum_phase<KBUF, DEG>(sc, C, ray, B, blockDim.x, slot, wstack, lane, act, L);
   } else {
     if (valid) L = resume_ray(P.out, r);
     act = valid;
   }
   const bool last = PASS == 2 || n < split_min;
-  act = run_rounds<KBUF, DEG>(sc, C, ray, B, blockDim.x, slot, wstack, lane, act, L, last ? INT_MAX : 1);
+  // after the frustum phase, pass 0 hands its few unfinished rays on without a round
+  const int rounds = last ? INT_MAX : (PASS == 0 && C.frustum ? 0 : 1);
+  act = run_rounds<KBUF, DEG>(sc, C, ray, B, blockDim.x, slot, wstack, lane, act, L, rounds);
   if (PASS < 2) {
     const unsigned m = __ballot_sync(kFull, act);
     if (lane == 0) mask[gi >> 5] = m;
@@ -656,12 +898,12 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value)
                        int64_t num_slots) {
   extern __shared__ int smem[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  int* wstack = smem + warp * kStackDepth;
-  float* B = reinterpret_cast<float*>(smem + (blockDim.x / 32) * kStackDepth) + tid;
+  int* wstack = smem + warp * kWarpInts;  // stack, then the frustum phase's lists
+  float* B = reinterpret_cast<float*>(smem + (blockDim.x / 32) * kWarpInts) + tid;
   const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;
   const int64_t p = gi < num_slots ? camera_slot_pixel(cam, gi) : -1;
   const bool valid = p >= 0;
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, num_slots, P.out};
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, num_slots, P.out, P.frustum != 0};
   float3 ro, rd;
   camera_ray(cam, jitter, valid ? p : 0, ro, rd);
   const Ray ray = make_ray(ro, rd, P.tmin);
@@ -674,9 +916,9 @@ template <int KBUF, int DEG, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value) k_trace_fwd_batched(const BatchFwdParams P) {
   extern __shared__ int smem[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  int* wstack = smem + warp * kStackDepth;
-  float* B = reinterpret_cast<float*>(smem + (blockDim.x / 32) * kStackDepth) + tid;
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.num_slots, P.out};
+  int* wstack = smem + warp * kWarpInts;  // stack, then the frustum phase's lists
+  float* B = reinterpret_cast<float*>(smem + (blockDim.x / 32) * kWarpInts) + tid;
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.num_slots, P.out, P.frustum != 0};
   const int64_t num_packets = P.num_slots / 32;
   for (;;) {
     unsigned int pk = 0;
@@ -695,6 +937,20 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value) k_trace_fwd
   }
 }
 
+// Dynamic shared memory of a packet kernel: per warp its stack and frustum-phase lists,
+// per thread the SH basis of its ray.
+template <int DEG>
+size_t packet_smem(int block) {
+  return size_t(kWarpInts) * (block / 32) * sizeof(int) + size_t((DEG + 1) * (DEG + 1)) * block * sizeof(float);
+}
+
+// Dynamic shared memory above the 48 KB default needs the kernel's opt-in.
+template <class Kern>
+cudaError_t prepare(Kern kern, size_t smem) {
+  if (smem <= size_t(48) * 1024) return cudaSuccess;
+  return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+}
+
 template <int KBUF, int DEG>
 cudaError_t launch_t(const FwdParams& P, int block, int traversal, cudaStream_t st) {
   const int64_t grid = (P.R + block - 1) / block;
@@ -705,11 +961,23 @@ cudaError_t launch_t(const FwdParams& P, int block, int traversal, cudaStream_t 
     if (e != cudaSuccess) return e;
     kern<<<unsigned(grid), block, smem, st>>>(P);
   } else {
-    const size_t smem = size_t(kStackDepth) * (block / 32) * sizeof(int) + size_t(16) * block * sizeof(float);
+    const size_t smem = packet_smem<DEG>(block);
     switch (block) {
-      case 64: k_trace_fwd_packet<KBUF, DEG, 64><<<unsigned(grid), 64, smem, st>>>(P); break;
-      case 128: k_trace_fwd_packet<KBUF, DEG, 128><<<unsigned(grid), 128, smem, st>>>(P); break;
-      default: k_trace_fwd_packet<KBUF, DEG, 256><<<unsigned(grid), 256, smem, st>>>(P); break;
+      case 64: {
+        if (cudaError_t e_ = prepare(k_trace_fwd_packet<KBUF, DEG, 64>, smem)) return e_;
+        k_trace_fwd_packet<KBUF, DEG, 64><<<unsigned(grid), 64, smem, st>>>(P);
+        break;
+      }
+      case 128: {
+        if (cudaError_t e_ = prepare(k_trace_fwd_packet<KBUF, DEG, 128>, smem)) return e_;
+        k_trace_fwd_packet<KBUF, DEG, 128><<<unsigned(grid), 128, smem, st>>>(P);
+        break;
+      }
+      default: {
+        if (cudaError_t e_ = prepare(k_trace_fwd_packet<KBUF, DEG, 256>, smem)) return e_;
+        k_trace_fwd_packet<KBUF, DEG, 256><<<unsigned(grid), 256, smem, st>>>(P);
+        break;
+      }
     }
   }
   return cudaGetLastError();
@@ -729,13 +997,16 @@ template <int KBUF, int DEG, int BLOCK, bool CAM>
 cudaError_t launch_regrouped_b(const FwdParams& P, const RegroupScratch& W, const PassCamera& Q, cudaStream_t st) {
   const int64_t n = CAM ? Q.num_slots : P.R;
   const unsigned grid = unsigned((n + BLOCK - 1) / BLOCK);
-  const size_t smem = size_t(kStackDepth) * (BLOCK / 32) * sizeof(int) + size_t(16) * BLOCK * sizeof(float);
+  const size_t smem = packet_smem<DEG>(BLOCK);
+  if (cudaError_t e_ = prepare(k_trace_fwd_pass<KBUF, DEG, BLOCK, 0, CAM>, smem)) return e_;
   k_trace_fwd_pass<KBUF, DEG, BLOCK, 0, CAM><<<grid, BLOCK, smem, st>>>(P, nullptr, nullptr, W.mask0, W.split_min, Q);
   cudaError_t e = regroup_compact(W.mask0, nullptr, n, nullptr, W.offsets, W.list1, W.count1, st);
   if (e != cudaSuccess) return e;
+  if (cudaError_t e_ = prepare(k_trace_fwd_pass<KBUF, DEG, BLOCK, 1, CAM>, smem)) return e_;
   k_trace_fwd_pass<KBUF, DEG, BLOCK, 1, CAM><<<grid, BLOCK, smem, st>>>(P, W.list1, W.count1, W.mask1, W.split_min, Q);
   e = regroup_compact(W.mask1, W.count1, n, W.list1, W.offsets, W.list2, W.count2, st);
   if (e != cudaSuccess) return e;
+  if (cudaError_t e_ = prepare(k_trace_fwd_pass<KBUF, DEG, BLOCK, 2, CAM>, smem)) return e_;
   k_trace_fwd_pass<KBUF, DEG, BLOCK, 2, CAM><<<grid, BLOCK, smem, st>>>(P, W.list2, W.count2, nullptr, 0, Q);
   return cudaGetLastError();
 }
@@ -778,11 +1049,23 @@ cudaError_t launch_camera_t(const FwdParams& P, const CameraParams& cam, const f
                             cudaStream_t st) {
   const int64_t num_slots = camera_slots(cam);
   const unsigned grid = unsigned((num_slots + block - 1) / block);
-  const size_t smem = size_t(kStackDepth) * (block / 32) * sizeof(int) + size_t(16) * block * sizeof(float);
+  const size_t smem = packet_smem<DEG>(block);
   switch (block) {
-    case 64: k_trace_fwd_camera<KBUF, DEG, 64><<<grid, 64, smem, st>>>(P, cam, jitter, num_slots); break;
-    case 128: k_trace_fwd_camera<KBUF, DEG, 128><<<grid, 128, smem, st>>>(P, cam, jitter, num_slots); break;
-    default: k_trace_fwd_camera<KBUF, DEG, 256><<<grid, 256, smem, st>>>(P, cam, jitter, num_slots); break;
+    case 64: {
+      if (cudaError_t e_ = prepare(k_trace_fwd_camera<KBUF, DEG, 64>, smem)) return e_;
+      k_trace_fwd_camera<KBUF, DEG, 64><<<grid, 64, smem, st>>>(P, cam, jitter, num_slots);
+      break;
+    }
+    case 128: {
+      if (cudaError_t e_ = prepare(k_trace_fwd_camera<KBUF, DEG, 128>, smem)) return e_;
+      k_trace_fwd_camera<KBUF, DEG, 128><<<grid, 128, smem, st>>>(P, cam, jitter, num_slots);
+      break;
+    }
+    default: {
+      if (cudaError_t e_ = prepare(k_trace_fwd_camera<KBUF, DEG, 256>, smem)) return e_;
+      k_trace_fwd_camera<KBUF, DEG, 256><<<grid, 256, smem, st>>>(P, cam, jitter, num_slots);
+      break;
+    }
   }
   return cudaGetLastError();
 }
@@ -800,13 +1083,25 @@ cudaError_t launch_camera_k(const FwdParams& P, const CameraParams& cam, const f
 
 template <int KBUF, int DEG>
 cudaError_t launch_batched_t(const BatchFwdParams& P, int block, cudaStream_t st) {
-  const size_t smem = size_t(kStackDepth) * (block / 32) * sizeof(int) + size_t(16) * block * sizeof(float);
+  const size_t smem = packet_smem<DEG>(block);
   cudaError_t e = cudaMemsetAsync(P.work_counter, 0, sizeof(unsigned int), st);
   if (e != cudaSuccess) return e;
   switch (block) {
-    case 64: k_trace_fwd_batched<KBUF, DEG, 64><<<P.grid, 64, smem, st>>>(P); break;
-    case 128: k_trace_fwd_batched<KBUF, DEG, 128><<<P.grid, 128, smem, st>>>(P); break;
-    default: k_trace_fwd_batched<KBUF, DEG, 256><<<P.grid, 256, smem, st>>>(P); break;
+    case 64: {
+      if (cudaError_t e_ = prepare(k_trace_fwd_batched<KBUF, DEG, 64>, smem)) return e_;
+      k_trace_fwd_batched<KBUF, DEG, 64><<<P.grid, 64, smem, st>>>(P);
+      break;
+    }
+    case 128: {
+      if (cudaError_t e_ = prepare(k_trace_fwd_batched<KBUF, DEG, 128>, smem)) return e_;
+      k_trace_fwd_batched<KBUF, DEG, 128><<<P.grid, 128, smem, st>>>(P);
+      break;
+    }
+    default: {
+      if (cudaError_t e_ = prepare(k_trace_fwd_batched<KBUF, DEG, 256>, smem)) return e_;
+      k_trace_fwd_batched<KBUF, DEG, 256><<<P.grid, 256, smem, st>>>(P);
+      break;
+    }
   }
   return cudaGetLastError();
 }

@@ -36,7 +36,7 @@ def _stream(device):
 class Tune:
     kbuf: int = 16
     block: int = 128
-    traversal: int = 0  # 0: warp packets, 1: one walk per ray
+    traversal: int = 0  # 0: warp packets with the frustum phase, 1: one walk per ray, 2: packets, rounds only
     regroup_min: int = 0  # regrouped forward: rays below which a pass runs every remaining round (0: auto)
 
     def c(self):
@@ -175,7 +175,7 @@ def forward(scene: Scene, rayo, rayd, tmin=0.0, tmax=1000.0, max_iters=500, sh_d
     with torch.cuda.device(device):
         # the packed passes pay for buffers of up to 16 events; with 32, most rays finish in
         # the first round and the extra passes only add their overhead
-        if regrouped and tune.traversal == 0 and tune.kbuf <= 16 and R < (1 << 31):
+        if regrouped and tune.traversal in (0, 2) and tune.kbuf <= 16 and R < (1 << 31):
             need = int(lib.ever_trace_forward_workspace_bytes(R))
             if workspace is None or workspace.numel() < need:
                 workspace = torch.empty(max(need, 256), dtype=torch.uint8, device=device)

