@@ -64,7 +64,7 @@ def test_small_uniform_sh0():
 
 
 @pytest.mark.parametrize("sh_degree", [None, 3])
-@pytest.mark.parametrize("traversal", [0, 1])
+@pytest.mark.parametrize("traversal", [0, 1, 2])
 @pytest.mark.parametrize("kbuf,block", [(8, 64), (16, 128), (32, 256)])
 def test_sh3_scene_all_launch_shapes(kbuf, block, traversal, sh_degree):
     sc = S.uniform_scene(3000, 3, seed=7)
@@ -115,6 +115,25 @@ def test_unnormalised_quats_and_directions():
     rd = (rd * rng.uniform(0.5, 2.0, (rd.shape[0], 1))).astype(np.float32)
     _, fwd, tri = _gpu_trace(sc, ro, rd, tmin=0.1)
     _assert_parity(fwd, tri, _oracle(sc, ro, rd, tmin=0.1))
+
+
+@pytest.mark.parametrize("traversal", [0, 2])
+def test_long_thin_tube_overflows_the_packet_lists(traversal):
+    # 3,000 small ellipsoids strung along the z axis and a packet of rays down the axis:
+    # the packet meets more leaves than its shared-memory list holds, so the frustum
+    # phase hands the whole packet to the gather rounds; results stay exact
+    rng = np.random.default_rng(17)
+    n = 3000
+    mean = np.stack([rng.normal(0, 0.01, n), rng.normal(0, 0.01, n), np.linspace(0.5, 20.0, n)], 1)
+    sc = S.SceneArrays(mean.astype(np.float32), np.full((n, 3), 0.02, np.float32),
+                       S.uniform_scene(n, 0, seed=17).quat, np.full((n, 1), 0.02, np.float32),
+                       rng.normal(0, 0.5, (n, 1, 3)).astype(np.float32))
+    ro = np.zeros((64, 3), np.float32)
+    ang = rng.uniform(-2e-3, 2e-3, (64, 2))
+    rd = np.stack([ang[:, 0], ang[:, 1], np.ones(64)], 1).astype(np.float32)
+    _, fwd, tri = _gpu_trace(sc, ro, rd, tune=T.Tune(traversal=traversal), max_iters=2000)
+    _assert_parity(fwd, tri, _oracle(sc, ro, rd, max_iters=2000))
+    assert int(fwd.iters.max()) > 100
 
 
 def test_duplicate_ellipsoids_round_boundary():
