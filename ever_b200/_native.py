@@ -50,7 +50,8 @@ class EverBatch(ctypes.Structure):
 
 
 class EverMlp(ctypes.Structure):
-    _fields_ = [("params", c_p), ("w1", c_p), ("w2", c_p), ("w3", c_p), ("centre", c_f32 * 3), ("inv_scale", c_f32)]
+    _fields_ = [("params", c_p), ("w1", c_p), ("w2", c_p), ("w3", c_p), ("centre", c_f32 * 3), ("inv_scale", c_f32),
+                ("wait_clocks", c_i64)]
 
 
 class EverCamera(ctypes.Structure):

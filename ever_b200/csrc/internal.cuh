@@ -253,6 +253,7 @@ struct MlpParams {
   float loss_w0, loss_w1, inv_batch;
   float* partial;  // (grid, kMlpParams + 1): per-CTA gradient and loss
   int32_t* error;  // set to 1 when a tensor-core wait times out
+  long long wait_clocks;  // bound of each tensor-core completion wait (0: about a second)
 };
 
 cudaError_t launch_mlp(const MlpParams& P, bool train, int max_grid, cudaStream_t st);

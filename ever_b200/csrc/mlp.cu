@@ -91,11 +91,30 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t phase) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait (2^31 clocks, about a second); false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\tmbarrier.test_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+
+constexpr long long kWaitClocks = 1ll << 31;  // about a second
+// Bounded wait for phase `phase` of the barrier; false once `limit` clocks have passed.
+// Shorter limits than the default poll with the non-blocking test (a try_wait may itself
+// suspend for longer than such a limit), so a test can make a wait run out for certain.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, long long limit = kWaitClocks) {
   const long long t0 = clock64();
+  if (limit < kWaitClocks) {
+    while (!mbar_test(bar, phase))
+      if (clock64() - t0 > limit) return false;
+    return true;
+  }
   while (!mbar_try(bar, phase))
-    if (clock64() - t0 > (1ll << 31)) return false;
+    if (clock64() - t0 > limit) return false;
   return true;
 }
 
@@ -264,7 +283,7 @@ __global__ void __launch_bounds__(128, TRAIN ? 1 : kInferCtasPerSm) k_mlp(const 
       mma_commit(&S.bar);
     }
     pending = phase;
-    const bool got = mbar_wait(&S.bar, phase);
+    const bool got = mbar_wait(&S.bar, phase, P.wait_clocks > 0 ? P.wait_clocks : kWaitClocks);
     phase ^= 1u;
     tc_fence_after();
     return __syncthreads_and(got) != 0;
@@ -457,7 +476,8 @@ __global__ void __launch_bounds__(128, TRAIN ? 1 : kInferCtasPerSm) k_mlp(const 
     if (tid == 0) out[kMlpParams] = ((S.loss[0] + S.loss[1]) + S.loss[2]) + S.loss[3];
   }
   if (!ok) {
-    mbar_wait(&S.bar, pending);  // let MMAs still in flight finish (bounded) before TMEM is freed
+    // let MMAs still in flight finish (bounded, at the full limit) before TMEM is freed
+    mbar_wait(&S.bar, pending, kWaitClocks);
     if (tid == 0) atomicExch(P.error, 1);
   }
   tc_fence_before();

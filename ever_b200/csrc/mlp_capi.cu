@@ -32,6 +32,7 @@ ever::MlpParams base_params(const EverMlp* m) {
   P.cy = m->centre[1];
   P.cz = m->centre[2];
   P.inv_scale = m->inv_scale;
+  P.wait_clocks = m->wait_clocks;
   return P;
 }
 

@@ -89,6 +89,13 @@ class CostModel:
         if int(self.error.item()) != 0:
             raise RuntimeError("ever_b200: tensor-core wait timed out in the cost model")
 
+    def clear_error(self):
+        self.error.zero_()
+
+    def set_wait_clocks(self, clocks: int = 0):
+        """Bound of each wait for the tensor cores in clocks (0: the default, about a second)."""
+        self._s.wait_clocks = int(clocks)
+
     @staticmethod
     def _rays(rayo, rayd):
         for t in (rayo, rayd):

@@ -306,6 +306,9 @@ typedef struct EverMlp {
   void* w3;
   float centre[3];  /* scene centre of the encoding */
   float inv_scale;  /* 1 / scene scale of the encoding */
+  int64_t wait_clocks; /* bound in clocks of each wait for the tensor cores (0: 2^31, about a
+                          second); a wait that runs out sets *error, lets the MMAs in flight
+                          finish and frees the tensor memory. Tests set a few clocks. */
 } EverMlp;
 
 /* Bytes of workspace ever_mlp_gradients needs (per-CTA partial gradients). */

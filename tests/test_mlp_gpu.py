@@ -89,6 +89,35 @@ def _ray_problem(R, seed):
     return p, ro, rd, target
 
 
+@pytest.mark.parametrize("train", [False, True])
+def test_tensor_core_wait_that_runs_out_is_reported_and_the_next_call_succeeds(train):
+    # A wait bound of a few clocks makes the first completion wait give up while the MMAs are
+    # still running: the kernel raises the error word, lets the MMAs in flight finish (at the
+    # full bound) and frees its tensor memory, so the context stays usable and a call with
+    # the default bound right after gives the exact results.
+    dev = _dev()
+    p, feat, target = _dyadic_problem(4096, 7)
+    cm = SCH.CostModel(params=p, device=dev)
+    x = torch.tensor(feat, device=dev)
+    run = (lambda: cm.gradients(None, None, torch.tensor(target, device=dev), feat=x)) if train else (
+        lambda: cm.predict(feat=x))
+    cm.set_wait_clocks(4)
+    run()
+    torch.cuda.synchronize()
+    with pytest.raises(RuntimeError, match="timed out"):
+        cm.check()
+    cm.clear_error()
+    cm.set_wait_clocks(0)
+    out = run()
+    torch.cuda.synchronize()
+    cm.check()
+    if train:
+        ref, _ = M.gradients(p, feat, target, 1.0, 1.0)
+        assert max(_block_errors(out[0].cpu().numpy().astype(np.float64), ref).values()) < 1e-5
+    else:
+        np.testing.assert_array_equal(out[0].cpu().numpy(), M.predict(p, feat))
+
+
 def test_predictions_on_encoded_rays_match_oracle():
     dev = _dev()
     p, ro, rd, _ = _ray_problem(30_000, 3)
