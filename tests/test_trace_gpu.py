@@ -118,22 +118,46 @@ def test_unnormalised_quats_and_directions():
 
 
 @pytest.mark.parametrize("traversal", [0, 2])
-def test_long_thin_tube_overflows_the_packet_lists(traversal):
-    # 3,000 small ellipsoids strung along the z axis and a packet of rays down the axis:
-    # the packet meets more leaves than its shared-memory list holds, so the frustum
-    # phase hands the whole packet to the gather rounds; results stay exact
+def test_long_row_of_ellipsoids_overflows_the_packet_lists(traversal):
+    # 1,200 disjoint small ellipsoids in a row along the z axis and a packet of rays down the
+    # row: the packet can meet more leaves than its shared-memory list holds, so the frustum
+    # phase hands the whole packet to the gather rounds; the results stay exact. (Disjoint
+    # and spaced, so no two events of a ray share a t: the oracle orders such ties by index,
+    # the GPU by Morton position.)
     rng = np.random.default_rng(17)
-    n = 3000
-    mean = np.stack([rng.normal(0, 0.01, n), rng.normal(0, 0.01, n), np.linspace(0.5, 20.0, n)], 1)
+    n = 1200
+    mean = np.stack([rng.uniform(-2e-3, 2e-3, n), rng.uniform(-2e-3, 2e-3, n), 0.5 + 0.05 * np.arange(n)], 1)
     sc = S.SceneArrays(mean.astype(np.float32), np.full((n, 3), 0.02, np.float32),
-                       S.uniform_scene(n, 0, seed=17).quat, np.full((n, 1), 0.02, np.float32),
+                       S.uniform_scene(n, 0, seed=17).quat, np.full((n, 1), 0.01, np.float32),
                        rng.normal(0, 0.5, (n, 1, 3)).astype(np.float32))
     ro = np.zeros((64, 3), np.float32)
-    ang = rng.uniform(-2e-3, 2e-3, (64, 2))
+    ang = rng.uniform(-2e-4, 2e-4, (64, 2))
     rd = np.stack([ang[:, 0], ang[:, 1], np.ones(64)], 1).astype(np.float32)
-    _, fwd, tri = _gpu_trace(sc, ro, rd, tune=T.Tune(traversal=traversal), max_iters=2000)
-    _assert_parity(fwd, tri, _oracle(sc, ro, rd, max_iters=2000))
-    assert int(fwd.iters.max()) > 100
+    _, fwd, tri = _gpu_trace(sc, ro, rd, tune=T.Tune(traversal=traversal), max_iters=3000)
+    _assert_parity(fwd, tri, _oracle(sc, ro, rd, max_iters=3000))
+    assert int(fwd.iters.max()) > 1000
+    _, ref, tref = _gpu_trace(sc, ro, rd, tune=T.Tune(traversal=2), max_iters=3000)
+    assert torch.equal(fwd.out, ref.out) and torch.equal(fwd.states, ref.states) and np.array_equal(tri, tref)
+
+
+def test_nested_shells_overflow_the_pending_buffer_midway():
+    # 24 nested ellipsoids: a ray meets 24 entries before the first exit, so its 16-event
+    # buffer overflows after some of the entries have been integrated; the rounds then
+    # continue the ray from its last integrated event. Exact against the oracle and equal
+    # bit for bit to the rounds-only mode.
+    rng = np.random.default_rng(23)
+    n = 24
+    r = np.linspace(0.1, 1.2, n)
+    sc = S.SceneArrays(rng.normal(0, 0.01, (n, 3)).astype(np.float32),
+                       (r[:, None] * rng.uniform(0.9, 1.1, (n, 3))).astype(np.float32),
+                       S.uniform_scene(n, 0, seed=23).quat, rng.uniform(0.05, 0.2, (n, 1)).astype(np.float32),
+                       rng.normal(0, 0.5, (n, 1, 3)).astype(np.float32))
+    ro, rd = S.look_at_rays(S.Camera(np.array([0.2, -0.1, 3.0]), 16, 16, 20.0))
+    _, fwd, tri = _gpu_trace(sc, ro, rd)
+    _assert_parity(fwd, tri, _oracle(sc, ro, rd))
+    assert int(fwd.iters.max()) >= 30
+    _, ref, tref = _gpu_trace(sc, ro, rd, tune=T.Tune(traversal=2))
+    assert torch.equal(fwd.out, ref.out) and torch.equal(fwd.states, ref.states) and np.array_equal(tri, tref)
 
 
 def test_duplicate_ellipsoids_round_boundary():
