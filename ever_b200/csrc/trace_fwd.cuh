@@ -705,6 +705,10 @@ __device__ bool frustum_phase(const SceneRef& sc, const TraceCtx& C, const Ray& 
   for (int i = 0; i < KBUF; ++i) buf[i] = kEmptyKey;
   bool live = act;  // still integrating in this phase
   for (int ci = 0;; ++ci) {
+    // every 32 leaves, the lanes start the loads of the next 32 records into L1 (one each),
+    // so the broadcast record loads of the loop below rarely wait on L2
+    if ((ci & 31) == 0 && ci + lane < nc)
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(sc.recs + int(uint32_t(cand[ci + lane]))));
     const uint64_t ck = ci < nc ? cand[ci] : kEmptyKey;
     const float T = ci < nc ? key_t(ck) : INFINITY;
     // events below T are final: no leaf still to come has an event before T
