@@ -21,7 +21,7 @@ class EverScene(ctypes.Structure):
 
 class EverTune(ctypes.Structure):
     _fields_ = [("kbuf", c_i32), ("block", c_i32), ("traversal", c_i32), ("regroup_min", c_i32),
-                ("reserved", c_i32 * 4)]
+                ("stack_depth", c_i32), ("reserved", c_i32 * 3)]
 
 
 class EverForwardOut(ctypes.Structure):

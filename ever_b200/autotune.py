@@ -1,14 +1,17 @@
 """Autotuner for the trace launch configuration.
 
-Tunables: the event buffer gathered per traversal round (kbuf 8/16/32), the block shape
-(64/128/256 threads: 2/4/8 warp packets per block), the traversal (warp packets or one
-walk per ray) and whether rays are reordered into coherent packets. The traversal stack
-is one 64-entry stack per warp in shared memory (256 B), too small to be worth tuning.
+Tunables: the event buffer (kbuf 8/16/32: gathered per round, and the frustum phase's
+per-ray buffer), the block shape (64/128/256 threads: 2/4/8 warp packets per block), the
+traversal (warp packets with the frustum phase, one walk per ray, or warp packets with
+gather rounds only), the traversal stack depth (entries in use, 8..64) and whether rays are
+reordered into coherent packets.
 
 Each candidate runs the caller's workload (one forward + backward) under CUDA events;
-the fastest one that finishes without a status flag wins. Results are cached in a JSON
-file keyed by GPU name, SH coefficients and power-of-two buckets of the ellipsoid and
-ray counts.
+the fastest one that finishes without a status flag wins: a stack too shallow for the
+tree raises EVER_STATUS_STACK_OVERFLOW and is rejected. Results are cached in a JSON file
+keyed by GPU name, SH coefficients and power-of-two buckets of the ellipsoid and ray
+counts; trace_rays looks its workload's key up there (cached_tune) and runs the cached pick
+when there is one.
 """
 from __future__ import annotations
 
@@ -29,13 +32,19 @@ class Candidate:
     block: int
     traversal: int = 0
     ordered: bool = True
+    stack_depth: int = 64
 
     def tune(self) -> Tune:
-        return Tune(kbuf=self.kbuf, block=self.block, traversal=self.traversal)
+        return Tune(kbuf=self.kbuf, block=self.block, traversal=self.traversal, stack_depth=self.stack_depth)
+
+    def name(self) -> str:
+        return (f"k{self.kbuf}-b{self.block}-t{self.traversal}-s{self.stack_depth}-"
+                f"{'ord' if self.ordered else 'idx'}")
 
 
-DEFAULT_CANDIDATES = [Candidate(k, b, 0, True) for k in (8, 16, 32) for b in (64, 128, 256)] + [
-    Candidate(16, 128, 0, False), Candidate(16, 128, 1, True)]
+DEFAULT_CANDIDATES = ([Candidate(k, b, 0, True) for k in (8, 16, 32) for b in (64, 128, 256)] +
+                      [Candidate(16, 128, 2, True), Candidate(16, 128, 0, False), Candidate(16, 128, 1, True)] +
+                      [Candidate(16, 128, 0, True, d) for d in (16, 24, 32, 48)])
 
 
 def default_cache_path() -> str:
@@ -72,12 +81,11 @@ def autotune(run: Callable[[Candidate], int], key: str, candidates: Iterable[Can
     cache_path = cache_path or default_cache_path()
     cache = _load(cache_path)
     if not force and key in cache:
-        c = cache[key]
-        return Candidate(c["kbuf"], c["block"], c["traversal"], c["ordered"]), c.get("timings", {})
+        return _from_entry(cache[key]), cache[key].get("timings", {})
     timings = {}
     best, best_ms = None, float("inf")
     for cand in candidates:
-        name = f"k{cand.kbuf}-b{cand.block}-t{cand.traversal}-{'ord' if cand.ordered else 'idx'}"
+        name = cand.name()
         try:
             for _ in range(warmup):
                 run(cand)
@@ -101,3 +109,13 @@ def autotune(run: Callable[[Candidate], int], key: str, candidates: Iterable[Can
     cache[key] = dict(asdict(best), ms=best_ms, timings=timings)
     _store(cache_path, cache)
     return best, timings
+
+
+def _from_entry(c) -> Candidate:
+    return Candidate(c["kbuf"], c["block"], c["traversal"], c["ordered"], c.get("stack_depth", 64))
+
+
+def cached_tune(num_prims: int, num_rays: int, sh_coeffs: int, device=None, cache_path: str | None = None):
+    """The cached pick for this workload's key (no timing run), or None."""
+    entry = _load(cache_path or default_cache_path()).get(workload_key(num_prims, num_rays, sh_coeffs, device))
+    return _from_entry(entry) if entry else None

@@ -32,6 +32,7 @@ EverTune resolve_tune(const EverTune* t) {
   if (t) r = *t;
   if (r.kbuf != 8 && r.kbuf != 16 && r.kbuf != 32) r.kbuf = 16;
   if (r.block != 64 && r.block != 128 && r.block != 256) r.block = 128;
+  r.stack_depth = r.stack_depth <= 0 ? ever::kStackDepth : std::min(std::max(r.stack_depth, 8), ever::kStackDepth);
   return r;
 }
 

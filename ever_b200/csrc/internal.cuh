@@ -71,6 +71,7 @@ struct FwdParams {
   const int32_t* ray_order;
   EverForwardOut out;
   int frustum;  // packet kernels: frustum phase before the rounds (set from the tune)
+  int stack_depth;  // traversal stack entries in use, <= kStackDepth (set from the tune)
 };
 
 cudaError_t launch_forward(const FwdParams& P, int deg, const EverTune& tune, cudaStream_t st);
@@ -143,6 +144,7 @@ struct BatchFwdParams {
   unsigned int* work_counter;
   int grid;            // persistent blocks
   int frustum;         // frustum phase before the rounds (set from the tune)
+  int stack_depth;     // traversal stack entries in use (set from the tune)
 };
 
 cudaError_t launch_forward_batched(const BatchFwdParams& P, int deg, const EverTune& tune, cudaStream_t st);

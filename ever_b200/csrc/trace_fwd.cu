@@ -123,6 +123,7 @@ cudaError_t regroup_compact(const uint32_t* mask, const uint32_t* n_dev, int64_t
 FwdParams with_mode(const FwdParams& P0, const EverTune& tune) {
   FwdParams P = P0;
   P.frustum = tune.traversal == 0 ? 1 : 0;
+  P.stack_depth = tune.stack_depth > 0 ? std::min(tune.stack_depth, kStackDepth) : kStackDepth;
   return P;
 }
 
@@ -153,6 +154,7 @@ cudaError_t launch_forward_regrouped(const FwdParams& P0, const RegroupScratch& 
 cudaError_t launch_forward_batched(const BatchFwdParams& P0, int deg, const EverTune& tune, cudaStream_t st) {
   BatchFwdParams P = P0;
   P.frustum = tune.traversal == 2 ? 0 : 1;
+  P.stack_depth = tune.stack_depth > 0 ? std::min(tune.stack_depth, kStackDepth) : kStackDepth;
   if (P.num_slots == 0) return cudaSuccess;
   const int block = tune.block > 0 ? tune.block : 128;
   switch (tune.kbuf) {

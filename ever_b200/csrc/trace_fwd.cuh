@@ -103,7 +103,7 @@ __device__ __forceinline__ void leaf_insert(const Record* __restrict__ recs, int
 template <int KBUF>
 __device__ void gather_ray(const Node* __restrict__ nodes, const Record* __restrict__ recs, const Ray& ray,
                            const RaySlab& sl, uint64_t lower, float s16, float tmax, uint64_t (&buf)[KBUF],
-                           int* st_node, float* st_t, int stride, uint32_t& status) {
+                           int* st_node, float* st_t, int stride, int depth, uint32_t& status) {
   const float lo_t = fmaxf(lower ? key_t(lower) : 0.f, s16);
   const float cap = fminf(tmax, kSentinel);
   int sp = 0;
@@ -121,7 +121,7 @@ __device__ void gather_ray(const Node* __restrict__ nodes, const Record* __restr
     const bool i1 = tc[1] != INFINITY && c[1] >= 0;
     if (i0 && i1) {
       const bool first0 = tc[0] <= tc[1];
-      if (sp < kStackDepth) {
+      if (sp < depth) {
         st_node[sp * stride] = first0 ? c[1] : c[0];
         st_t[sp * stride] = first0 ? tc[1] : tc[0];
         ++sp;
@@ -152,7 +152,7 @@ __device__ void gather_ray(const Node* __restrict__ nodes, const Record* __restr
 template <int KBUF>
 __device__ void gather_packet(const Node* __restrict__ nodes, const Record* __restrict__ recs, const Ray& ray,
                               const RaySlab& sl, bool act, uint64_t lower, float s16, float tmax,
-                              uint64_t (&buf)[KBUF], int* wstack, int lane, uint32_t& status) {
+                              uint64_t (&buf)[KBUF], int* wstack, int lane, int depth, uint32_t& status) {
   const float lo_t = fmaxf(lower ? key_t(lower) : 0.f, s16);
   const float cap = fminf(tmax, kSentinel);
   int sp = 0;
@@ -175,7 +175,7 @@ __device__ void gather_packet(const Node* __restrict__ nodes, const Record* __re
       // nearer child first, by majority of the lanes that hit either
       const unsigned pref0 = __ballot_sync(kFull, t0 <= t1 && t0 != INFINITY);
       const bool first0 = 2 * __popc(pref0) >= __popc(m0 | m1);
-      if (sp < kStackDepth) {
+      if (sp < depth) {
         if (lane == 0) {
           const int far = first0 ? c1 : c0;
           wstack[sp] = far;
@@ -242,8 +242,8 @@ template <int DEG, bool PACKET>
 __device__ int point_members(const Node* __restrict__ nodes, const Record* __restrict__ recs,
                              const int32_t* __restrict__ order, const float* __restrict__ feats, int fst,
                              const float* B, int bs, const Ray& ray, bool act,
-                             int* stack, int stride, int lane, int (&mem_p)[kMaxMembers], int (&mem_j)[kMaxMembers],
-                             float4& extra, uint32_t& status) {
+                             int* stack, int stride, int depth, int lane, int (&mem_p)[kMaxMembers],
+                             int (&mem_j)[kMaxMembers], float4& extra, uint32_t& status) {
   int n_mem = 0;
   int sp = 0;
   int node = 0;
@@ -260,7 +260,7 @@ __device__ int point_members(const Node* __restrict__ nodes, const Record* __res
       g1 = __any_sync(kFull, g1);
     }
     if (g0 && g1) {
-      if (sp < kStackDepth) {
+      if (sp < depth) {
         if (!PACKET || lane == 0) stack[sp * stride] = c1;
         ++sp;
       } else {
@@ -295,6 +295,7 @@ struct TraceCtx {
   int64_t log_stride;  // event-log row length (slots)
   EverForwardOut out;
   bool frustum;        // packet kernels: run the frustum phase before the rounds
+  int depth;           // traversal stack entries in use (<= kStackDepth)
 };
 
 // One event of a ray's sorted sequence, integrated under the reference's round rules
@@ -424,7 +425,7 @@ __global__ void __launch_bounds__(256) k_trace_fwd_ray(const FwdParams P) {
   if (gi >= P.R) return;
   const int64_t r = P.ray_order ? int64_t(P.ray_order[gi]) : gi;
   const SceneRef sc = scene_of(P);
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out, P.frustum != 0};
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out, P.frustum != 0, P.stack_depth};
   const Ray ray = load_ray(P.rayo, P.rayd, r, P.tmin);
   const RaySlab sl = make_slab(ray);
   float B[16];
@@ -438,7 +439,7 @@ __global__ void __launch_bounds__(256) k_trace_fwd_ray(const FwdParams P) {
     float4 extra = make_float4(0.f, 0.f, 0.f, 0.f);
     const int n_mem = point_members<DEG, false>(sc.nodes, sc.recs, sc.order, sc.features, feat_stride(sc.K), B, 1,
                                                 ray, true,
-                                                st_node, stride, 0, mem_p, mem_j, extra, status);
+                                                st_node, stride, C.depth, 0, mem_p, mem_j, extra, status);
     init_density<DEG>(sc, B, 1, n_mem, mem_j, extra, status, s);
     float s16 = 0.f;
     int cnt16 = 0;
@@ -448,7 +449,8 @@ __global__ void __launch_bounds__(256) k_trace_fwd_ray(const FwdParams P) {
       uint64_t buf[KBUF];
 #pragma unroll
       for (int i = 0; i < KBUF; ++i) buf[i] = kEmptyKey;
-      gather_ray<KBUF>(sc.nodes, sc.recs, ray, sl, lower, s16, C.tmax, buf, st_node, st_t, stride, status);
+      gather_ray<KBUF>(sc.nodes, sc.recs, ray, sl, lower, s16, C.tmax, buf, st_node, st_t, stride, C.depth,
+                       status);
       done = consume<KBUF, DEG>(sc, C, ray, B, 1, gi, buf, s, last_dirac, iters, s16, cnt16, lower, status);
     }
   }
@@ -478,7 +480,8 @@ struct RayLoop {
 
 // Initial state of a ray: empty, plus the density of the ellipsoids its start lies in.
 template <int DEG>
-__device__ __forceinline__ RayLoop start_ray(const SceneRef& sc, const Ray& ray, bool valid, int* wstack, float* B,
+__device__ __forceinline__ RayLoop start_ray(const SceneRef& sc, const Ray& ray, bool valid, int* wstack, int depth,
+                                             float* B,
                                              int bs, int lane) {
   RayLoop L;
   L.status = 0;
@@ -493,7 +496,7 @@ __device__ __forceinline__ RayLoop start_ray(const SceneRef& sc, const Ray& ray,
     float4 extra = make_float4(0.f, 0.f, 0.f, 0.f);
     const int n_mem = point_members<DEG, true>(sc.nodes, sc.recs, sc.order, sc.features, feat_stride(sc.K), B, bs,
                                                ray, valid,
-                                               wstack, 1, lane, mem_p, mem_j, extra, L.status);
+                                               wstack, 1, depth, lane, mem_p, mem_j, extra, L.status);
     init_density<DEG>(sc, B, bs, n_mem, mem_j, extra, L.status, L.s);
   }
   return L;
@@ -509,7 +512,8 @@ __device__ __forceinline__ bool run_rounds(const SceneRef& sc, const TraceCtx& C
     uint64_t buf[KBUF];
 #pragma unroll
     for (int i = 0; i < KBUF; ++i) buf[i] = kEmptyKey;
-    gather_packet<KBUF>(sc.nodes, sc.recs, ray, sl, act, L.lower, L.s16, C.tmax, buf, wstack, lane, L.status);
+    gather_packet<KBUF>(sc.nodes, sc.recs, ray, sl, act, L.lower, L.s16, C.tmax, buf, wstack, lane, C.depth,
+                        L.status);
     if (act)
       act = !consume<KBUF, DEG>(sc, C, ray, B, bs, slot, buf, L.s, L.last_dirac, L.iters, L.s16, L.cnt16, L.lower,
                                 L.status);
@@ -753,7 +757,7 @@ template <int KBUF, int DEG>
 __device__ __forceinline__ void trace_packet(const SceneRef& sc, const TraceCtx& C, const Ray& ray, int64_t r,
                                              bool valid, int64_t slot, int* wstack, float* B, int bs, int lane) {
   store_basis<DEG>(ray, B, bs);
-  RayLoop L = start_ray<DEG>(sc, ray, valid, wstack, B, bs, lane);
+  RayLoop L = start_ray<DEG>(sc, ray, valid, wstack, C.depth, B, bs, lane);
   bool act = valid && C.max_iters > 0 && sc.N > 0;
   if (C.frustum) act = frustum_phase<KBUF, DEG>(sc, C, ray, B, bs, slot, wstack, lane, act, L);
   run_rounds<KBUF, DEG>(sc, C, ray, B, bs, slot, wstack, lane, act, L, INT_MAX);
@@ -813,7 +817,7 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value) k_trace_fwd
   const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;
   const bool valid = gi < P.R;  // every lane stays for the warp-wide ballots
   const int64_t r = valid ? (P.ray_order ? int64_t(P.ray_order[gi]) : gi) : 0;
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out, P.frustum != 0};
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out, P.frustum != 0, P.stack_depth};
   const Ray ray = load_ray(P.rayo, P.rayd, r, P.tmin);
   trace_packet<KBUF, DEG>(scene_of(P), C, ray, r, valid, gi, wstack, B, blockDim.x, lane);
 }
@@ -857,7 +861,7 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value)
   }
   if (!valid) r = 0;
   const SceneRef sc = scene_of(P);
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, slots, P.out, P.frustum != 0};
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, slots, P.out, P.frustum != 0, P.stack_depth};
   Ray ray;
   if (CAM) {
     float3 ro, rd;
@@ -870,7 +874,7 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value)
   RayLoop L;
   bool act;
   if (PASS == 0) {
-    L = start_ray<DEG>(sc, ray, valid, wstack, B, blockDim.x, lane);
+    L = start_ray<DEG>(sc, ray, valid, wstack, C.depth, B, blockDim.x, lane);
     act = valid && C.max_iters > 0 && sc.N > 0;
     if (C.frustum) act = frustum_phase<KBUF, DEG>(sc, C, ray, B, blockDim.x, slot, wstack, lane, act, L);
   } else {
@@ -907,7 +911,7 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value)
   const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;
   const int64_t p = gi < num_slots ? camera_slot_pixel(cam, gi) : -1;
   const bool valid = p >= 0;
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, num_slots, P.out, P.frustum != 0};
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, num_slots, P.out, P.frustum != 0, P.stack_depth};
   float3 ro, rd;
   camera_ray(cam, jitter, valid ? p : 0, ro, rd);
   const Ray ray = make_ray(ro, rd, P.tmin);
@@ -922,7 +926,7 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value) k_trace_fwd
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   int* wstack = smem + warp * kWarpInts;  // stack, then the frustum phase's lists
   float* B = reinterpret_cast<float*>(smem + (blockDim.x / 32) * kWarpInts) + tid;
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.num_slots, P.out, P.frustum != 0};
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.num_slots, P.out, P.frustum != 0, P.stack_depth};
   const int64_t num_packets = P.num_slots / 32;
   for (;;) {
     unsigned int pk = 0;

@@ -80,6 +80,15 @@ class SplineTracer(Function):
         ray_order="auto",
     ):
         ctx.device = rayo.device
+        if tune is None:  # the autotuner's cached pick for this workload, if it ran on it
+            from .autotune import cached_tune
+            pick = cached_tune(mean.shape[0], rayo.shape[0], color.shape[1], rayo.device)
+            if pick is not None:
+                # the full stack depth stays: the pick's depth was clean on the tuned scene, and
+                # a deeper tree in the same size bucket must not lose subtrees
+                tune = T.Tune(kbuf=pick.kbuf, block=pick.block, traversal=pick.traversal)
+                if not pick.ordered and isinstance(ray_order, str):
+                    ray_order = None
         scene = T.Scene(mean, scale, quat, density, color)
         needs_grad = any(ctx.needs_input_grad[:7]) or (mean2D is not None and ctx.needs_input_grad[10])
         if isinstance(ray_order, str):

@@ -38,10 +38,12 @@ class Tune:
     block: int = 128
     traversal: int = 0  # 0: warp packets with the frustum phase, 1: one walk per ray, 2: packets, rounds only
     regroup_min: int = 0  # regrouped forward: rays below which a pass runs every remaining round (0: auto)
+    stack_depth: int = 0  # traversal stack entries in use, 8..64 (0: 64)
 
     def c(self):
         t = N.EverTune()
         t.kbuf, t.block, t.traversal, t.regroup_min = self.kbuf, self.block, self.traversal, self.regroup_min
+        t.stack_depth = self.stack_depth
         return t
 
 

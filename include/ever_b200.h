@@ -61,7 +61,9 @@ typedef struct EverTune {
   int32_t regroup_min;/* ever_trace_forward_regrouped: a pass with fewer rays than this runs every
                          remaining round instead of handing the rest on; 0: four times the GPU's
                          resident lanes */
-  int32_t reserved[4];
+  int32_t stack_depth;/* traversal stack entries in use, 8..64 (0: 64); a tree deeper than the stack
+                         raises EVER_STATUS_STACK_OVERFLOW (a subtree is skipped) */
+  int32_t reserved[3];
 } EverTune;
 
 /* Per-ray outputs of a forward trace. Null pointers are skipped unless noted. */
