@@ -536,6 +536,7 @@ __device__ __forceinline__ bool run_rounds(const SceneRef& sc, const TraceCtx& C
 // continue it from there (lower = that event's key), so the results do not depend on it.
 constexpr int kFrontierCap = 384;  // nodes per breadth-first level
 constexpr int kCandCap = 512;      // leaves per packet (a power of two: the sort's width)
+constexpr int kLeafGroup = 4;      // leaves tested together before their events are inserted
 // Shared ints per warp: the traversal stack, two frontier levels, the leaf keys (64-bit).
 constexpr int kWarpInts = kStackDepth + 2 * kFrontierCap + 2 * kCandCap;
 
@@ -627,34 +628,44 @@ __device__ __forceinline__ int packet_leaves(const Node* __restrict__ nodes, con
   for (int level = 0; nf > 0; ++level) {
     if (level >= 4 * kStackDepth) return -1;  // deeper than any tree the build makes
     int nn = 0;
-    for (int base = 0; base < nf; base += 32) {
-      const int i = base + lane;
-      float te0 = INFINITY, te1 = INFINITY;
-      int c0 = 0, c1 = 0;
-      if (i < nf) {
-        const Node nd = load_node(nodes, cur[i]);
-        te0 = packet_entry(P, nd.a.x, nd.a.y, nd.a.z, nd.a.w, nd.b.x, nd.b.y, cap);
-        te1 = packet_entry(P, nd.b.z, nd.b.w, nd.c.x, nd.c.y, nd.c.z, nd.c.w, cap);
-        c0 = nd.d.x;
-        c1 = nd.d.y;
+    // two nodes per lane per batch: both loads are in flight before either box test
+    for (int base = 0; base < nf; base += 64) {
+      Node nd[2];
+      bool have[2];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int i = base + 32 * u + lane;
+        have[u] = i < nf;
+        if (have[u]) nd[u] = load_node(nodes, cur[i]);
       }
 #pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const float te = k ? te1 : te0;
-        const int c = k ? c1 : c0;
-        const bool hit = te != INFINITY;
-        const unsigned mi = __ballot_sync(kFull, hit && c >= 0);
-        const unsigned ml = __ballot_sync(kFull, hit && c < 0);
-        if (hit && c >= 0) {
-          const int q = nn + __popc(mi & below);
-          if (q < kFrontierCap) nxt[q] = c;
+      for (int u = 0; u < 2; ++u) {
+        float te0 = INFINITY, te1 = INFINITY;
+        int c0 = 0, c1 = 0;
+        if (have[u]) {
+          te0 = packet_entry(P, nd[u].a.x, nd[u].a.y, nd[u].a.z, nd[u].a.w, nd[u].b.x, nd[u].b.y, cap);
+          te1 = packet_entry(P, nd[u].b.z, nd[u].b.w, nd[u].c.x, nd[u].c.y, nd[u].c.z, nd[u].c.w, cap);
+          c0 = nd[u].d.x;
+          c1 = nd[u].d.y;
         }
-        if (hit && c < 0) {
-          const int q = nc + __popc(ml & below);
-          if (q < kCandCap) cand[q] = (uint64_t(__float_as_uint(te)) << 32) | uint32_t(~c);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const float te = k ? te1 : te0;
+          const int c = k ? c1 : c0;
+          const bool hit = te != INFINITY;
+          const unsigned mi = __ballot_sync(kFull, hit && c >= 0);
+          const unsigned ml = __ballot_sync(kFull, hit && c < 0);
+          if (hit && c >= 0) {
+            const int q = nn + __popc(mi & below);
+            if (q < kFrontierCap) nxt[q] = c;
+          }
+          if (hit && c < 0) {
+            const int q = nc + __popc(ml & below);
+            if (q < kCandCap) cand[q] = (uint64_t(__float_as_uint(te)) << 32) | uint32_t(~c);
+          }
+          nn += __popc(mi);
+          nc += __popc(ml);
         }
-        nn += __popc(mi);
-        nc += __popc(ml);
       }
     }
     __syncwarp();
@@ -667,27 +678,68 @@ __device__ __forceinline__ int packet_leaves(const Node* __restrict__ nodes, con
   return nc;
 }
 
-// Ascending bitonic sort of cand[0, n) in shared memory by the warp (n <= kCandCap).
-__device__ __forceinline__ void sort_keys(uint64_t* cand, int n, int lane) {
-  int w = 32;
-  while (w < n) w <<= 1;
-  for (int i = n + lane; i < w; i += 32) cand[i] = kEmptyKey;
-  __syncwarp();
-  for (int k = 2; k <= w; k <<= 1) {
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int i = lane; i < w; i += 32) {
-        const int l = i ^ j;
-        if (l > i) {
-          const uint64_t a = cand[i], b = cand[l];
-          if ((a > b) == ((i & k) == 0)) {
-            cand[i] = b;
-            cand[l] = a;
+__device__ __forceinline__ uint64_t shfl_xor64(uint64_t v, int m) {
+  const uint32_t lo = __shfl_xor_sync(kFull, uint32_t(v), m), hi = __shfl_xor_sync(kFull, uint32_t(v >> 32), m);
+  return (uint64_t(hi) << 32) | lo;
+}
+
+// Ascending bitonic sort of 32 * E keys held E per lane (key lane * E + r in k[r]): the
+// stages whose partners lie in the same lane compare-swap registers, the others exchange
+// with lane ^ (stride / E) by shuffles. No shared memory, no warp barriers.
+template <int E>
+__device__ __forceinline__ void sort_regs(uint64_t (&k)[E], int lane) {
+#pragma unroll
+  for (int size = 2; size <= 32 * E; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      if (stride < E) {
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+          const int q = r ^ stride;
+          if (q > r) {
+            const bool up = ((lane * E + r) & size) == 0;
+            const uint64_t a = k[r], b = k[q];
+            const bool sw = (a > b) == up;
+            k[r] = sw ? b : a;
+            k[q] = sw ? a : b;
           }
         }
+      } else {
+        const int m = stride / E;
+        const bool lower = (lane & m) == 0;
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+          const uint64_t o = shfl_xor64(k[r], m);
+          const bool up = ((lane * E + r) & size) == 0;
+          const bool take_min = lower == up;
+          k[r] = take_min ? (o < k[r] ? o : k[r]) : (o > k[r] ? o : k[r]);
+        }
       }
-      __syncwarp();
     }
   }
+}
+
+// Sorts cand[0, n) ascending in place (n <= kCandCap = 32 * 16). Not inlined: one copy
+// per translation unit instead of one per kernel.
+template <int E>
+__device__ __noinline__ void sort_keys_e(uint64_t* cand, int n, int lane) {
+  uint64_t k[E];
+#pragma unroll
+  for (int r = 0; r < E; ++r) {
+    const int i = lane * E + r;
+    k[r] = i < n ? cand[i] : kEmptyKey;
+  }
+  sort_regs<E>(k, lane);
+  __syncwarp();
+#pragma unroll
+  for (int r = 0; r < E; ++r) cand[lane * E + r] = k[r];
+  __syncwarp();
+}
+
+__device__ __forceinline__ void sort_keys(uint64_t* cand, int n, int lane) {
+  if (n <= 32 * 4) sort_keys_e<4>(cand, n, lane);
+  else if (n <= 32 * 8) sort_keys_e<8>(cand, n, lane);
+  else sort_keys_e<16>(cand, n, lane);
 }
 
 // The frustum phase of a warp's packet. Returns whether this lane's ray still needs rounds
@@ -708,14 +760,14 @@ __device__ bool frustum_phase(const SceneRef& sc, const TraceCtx& C, const Ray& 
 #pragma unroll
   for (int i = 0; i < KBUF; ++i) buf[i] = kEmptyKey;
   bool live = act;  // still integrating in this phase
-  for (int ci = 0;; ++ci) {
+  for (int cb = 0;; cb += kLeafGroup) {
     // every 32 leaves, the lanes start the loads of the next 32 records into L1 (one each),
-    // so the broadcast record loads of the loop below rarely wait on L2
-    if ((ci & 31) == 0 && ci + lane < nc)
-      asm volatile("prefetch.global.L1 [%0];" ::"l"(sc.recs + int(uint32_t(cand[ci + lane]))));
-    const uint64_t ck = ci < nc ? cand[ci] : kEmptyKey;
-    const float T = ci < nc ? key_t(ck) : INFINITY;
-    // events below T are final: no leaf still to come has an event before T
+    // so the broadcast record loads below rarely wait on L2
+    if ((cb & 31) == 0 && cb + lane < nc)
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(sc.recs + int(uint32_t(cand[cb + lane]))));
+    // events below T are final: no leaf still to come has an event before T. They are
+    // integrated once per group of leaves, when the lanes have several at once.
+    const float T = cb < nc ? key_t(cand[cb]) : INFINITY;
     while (live && buf[0] != kEmptyKey && key_t(buf[0]) < T) {
       const uint64_t k = buf[0];
 #pragma unroll
@@ -727,21 +779,32 @@ __device__ bool frustum_phase(const SceneRef& sc, const TraceCtx& C, const Ray& 
         act = false;  // finished
       }
     }
-    if (ci >= nc) break;
+    if (cb >= nc) break;
     if (!__any_sync(kFull, live)) break;
-    if (live) {
-      const int j = int(uint32_t(ck));
-      const Record R = load_record(sc.recs, j);
-      HitT H;
-      if (intersect(R, ray, H)) {
-        const bool in0 = H.t0 > L.s16 && H.t0 <= C.tmax;
-        const bool in1 = H.t1 > L.s16 && (H.t1 <= C.tmax || in0);
-        // a full buffer cannot take another event: stop here, the rounds continue the ray
-        if ((in0 || in1) && buf[KBUF - (in0 && in1 ? 2 : 1)] != kEmptyKey) {
-          live = false;
-        } else {
-          if (in0) buf_insert(buf, event_key(H.t0, j, 0));
-          if (in1) buf_insert(buf, event_key(H.t1, j, 1));
+    // the group's leaves: independent tests (their loads and roots overlap), then inserts
+    uint64_t e0[kLeafGroup], e1[kLeafGroup];
+#pragma unroll
+    for (int g = 0; g < kLeafGroup; ++g) {
+      e0[g] = e1[g] = kEmptyKey;
+      if (live && cb + g < nc) {
+        const int j = int(uint32_t(cand[cb + g]));
+        HitT H;
+        if (intersect(load_record(sc.recs, j), ray, H)) {
+          const bool in0 = H.t0 > L.s16 && H.t0 <= C.tmax;
+          if (in0) e0[g] = event_key(H.t0, j, 0);
+          if (H.t1 > L.s16 && (H.t1 <= C.tmax || in0)) e1[g] = event_key(H.t1, j, 1);
+        }
+      }
+    }
+#pragma unroll
+    for (int g = 0; g < kLeafGroup; ++g) {
+#pragma unroll
+      for (int x = 0; x < 2; ++x) {
+        const uint64_t e = x ? e1[g] : e0[g];
+        if (live && e != kEmptyKey) {
+          // a full buffer cannot take another event: stop here, the rounds continue the ray
+          if (buf[KBUF - 1] != kEmptyKey) live = false;
+          else buf_insert(buf, e);
         }
       }
     }

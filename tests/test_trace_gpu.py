@@ -134,7 +134,14 @@ def test_long_row_of_ellipsoids_overflows_the_packet_lists(traversal):
     ang = rng.uniform(-2e-4, 2e-4, (64, 2))
     rd = np.stack([ang[:, 0], ang[:, 1], np.ones(64)], 1).astype(np.float32)
     _, fwd, tri = _gpu_trace(sc, ro, rd, tune=T.Tune(traversal=traversal), max_iters=3000)
-    _assert_parity(fwd, tri, _oracle(sc, ro, rd, max_iters=3000))
+    ref = _oracle(sc, ro, rd, max_iters=3000)
+    iters = fwd.iters.cpu().numpy()
+    np.testing.assert_array_equal(iters, ref.iters)
+    mask = np.arange(tri.shape[0])[:, None] < iters[None, :]
+    np.testing.assert_array_equal(np.where(mask, tri, -1), np.where(mask, ref.events, -1))
+    # 2,400 events per ray: the last-bit differences of CUDA's and libm's expf add up to
+    # a few 1e-5 of the colour over so many updates (1e-5 holds for the usual ~20 events)
+    np.testing.assert_allclose(fwd.out.cpu().numpy()[:, :4], ref.out[:, :4], rtol=2e-4, atol=1e-6)
     assert int(fwd.iters.max()) > 1000
     _, ref, tref = _gpu_trace(sc, ro, rd, tune=T.Tune(traversal=2), max_iters=3000)
     assert torch.equal(fwd.out, ref.out) and torch.equal(fwd.states, ref.states) and np.array_equal(tri, tref)
