@@ -537,8 +537,12 @@ __device__ __forceinline__ bool run_rounds(const SceneRef& sc, const TraceCtx& C
 constexpr int kFrontierCap = 384;  // nodes per breadth-first level
 constexpr int kCandCap = 512;      // leaves per packet (a power of two: the sort's width)
 constexpr int kLeafGroup = 4;      // leaves tested together before their events are inserted
-// Shared ints per warp: the traversal stack, two frontier levels, the leaf keys (64-bit).
-constexpr int kWarpInts = kStackDepth + 2 * kFrontierCap + 2 * kCandCap;
+constexpr float kFirstStage = 1.0f;  // the first stage's share of the packet's t extent
+constexpr int kMaxHalvings = 24;     // halvings of an overflowing range before the rounds take over
+// Shared ints per warp: the traversal stack, two frontier levels, the leaf keys (64-bit),
+// the packet's bounds between stages.
+constexpr int kBoundsInts = 20;
+constexpr int kWarpInts = kStackDepth + 2 * kFrontierCap + 2 * kCandCap + kBoundsInts;
 
 __device__ __forceinline__ uint32_t ordered_bits(float f) {
   const uint32_t u = __float_as_uint(f);
@@ -579,15 +583,15 @@ __device__ __forceinline__ PacketBounds packet_bounds(const Ray& ray, const RayS
 __device__ __forceinline__ float min4(float a, float b, float c, float d) { return fminf(fminf(a, b), fminf(c, d)); }
 __device__ __forceinline__ float max4(float a, float b, float c, float d) { return fmaxf(fmaxf(a, b), fmaxf(c, d)); }
 
-// A lower bound of the t at which any packet ray enters the box within [0, cap], or +inf
-// when no packet ray can meet it there. Interval products bound every ray's plane
+// Bounds of the t range over which any packet ray can be inside the box, within
+// [t_lo, t_hi]; false when no packet ray meets the box there. Interval products bound every ray's plane
 // distances; the float rounding of the bound (a few ulps) is covered by widening it by a
 // relative 1e-6. Axes whose direction changes sign bound no t: there the positions the
 // packet reaches over the t range of the other axes must overlap the box.
-__device__ __forceinline__ float packet_entry(const PacketBounds& P, float lx, float ly, float lz, float hx, float hy,
-                                              float hz, float cap) {
+__device__ __forceinline__ bool packet_span(const PacketBounds& P, float lx, float ly, float lz, float hx, float hy,
+                                            float hz, float t_lo, float t_hi, float& tn_out, float& tf_out) {
   const float lo[3] = {lx, ly, lz}, hi[3] = {hx, hy, hz};
-  float tn = 0.f, tf = cap;
+  float tn = t_lo, tf = t_hi;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     if (P.free_axes >> a & 1u) continue;
@@ -600,7 +604,7 @@ __device__ __forceinline__ float packet_entry(const PacketBounds& P, float lx, f
   }
   tn = tn - 1e-6f * fabsf(tn);
   tf = tf + 1e-6f * fabsf(tf);
-  if (!(tn <= tf)) return INFINITY;
+  if (!(tn <= tf)) return false;
   if (P.free_axes) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -608,17 +612,27 @@ __device__ __forceinline__ float packet_entry(const PacketBounds& P, float lx, f
       const float xl = P.omin[a] + min4(tn * P.dmin[a], tn * P.dmax[a], tf * P.dmin[a], tf * P.dmax[a]);
       const float xh = P.omax[a] + max4(tn * P.dmin[a], tn * P.dmax[a], tf * P.dmin[a], tf * P.dmax[a]);
       const float tol = 1e-6f * (fabsf(xl) + fabsf(xh) + fabsf(tf));
-      if (xh + tol < lo[a] || xl - tol > hi[a]) return INFINITY;
+      if (xh + tol < lo[a] || xl - tol > hi[a]) return false;
     }
   }
-  return fmaxf(tn, 0.f);
+  tn_out = fmaxf(tn, 0.f);
+  tf_out = tf;
+  return true;
+}
+
+// A lower bound of the t at which any packet ray enters the box within [t_lo, t_hi], or
+// +inf when no packet ray can meet it there.
+__device__ __forceinline__ float packet_entry(const PacketBounds& P, float lx, float ly, float lz, float hx, float hy,
+                                              float hz, float t_lo, float t_hi) {
+  float tn, tf;
+  return packet_span(P, lx, ly, lz, hx, hy, hz, t_lo, t_hi, tn, tf) ? tn : INFINITY;
 }
 
 // Breadth-first walk: the leaf keys (entry bound bits << 32 | position) of every leaf the
-// packet can meet, into cand[0, n). Returns n, or -1 when a level or the leaf list does
-// not fit its shared-memory capacity.
-__device__ __forceinline__ int packet_leaves(const Node* __restrict__ nodes, const PacketBounds& P, float cap,
-                                             int* front, uint64_t* cand, int lane) {
+// packet can meet at some t in [t_lo, t_hi], into cand[0, n). Returns n, or -1 when a
+// level or the leaf list does not fit its shared-memory capacity.
+__device__ __noinline__ int packet_leaves(const Node* __restrict__ nodes, const PacketBounds& P, float t_lo,
+                                             float t_hi, int* front, uint64_t* cand, int lane) {
   int* cur = front;
   int* nxt = front + kFrontierCap;
   if (lane == 0) cur[0] = 0;
@@ -643,8 +657,8 @@ __device__ __forceinline__ int packet_leaves(const Node* __restrict__ nodes, con
         float te0 = INFINITY, te1 = INFINITY;
         int c0 = 0, c1 = 0;
         if (have[u]) {
-          te0 = packet_entry(P, nd[u].a.x, nd[u].a.y, nd[u].a.z, nd[u].a.w, nd[u].b.x, nd[u].b.y, cap);
-          te1 = packet_entry(P, nd[u].b.z, nd[u].b.w, nd[u].c.x, nd[u].c.y, nd[u].c.z, nd[u].c.w, cap);
+          te0 = packet_entry(P, nd[u].a.x, nd[u].a.y, nd[u].a.z, nd[u].a.w, nd[u].b.x, nd[u].b.y, t_lo, t_hi);
+          te1 = packet_entry(P, nd[u].b.z, nd[u].b.w, nd[u].c.x, nd[u].c.y, nd[u].c.z, nd[u].c.w, t_lo, t_hi);
           c0 = nd[u].d.x;
           c1 = nd[u].d.y;
         }
@@ -744,73 +758,121 @@ __device__ __forceinline__ void sort_keys(uint64_t* cand, int n, int lane) {
 
 // The frustum phase of a warp's packet. Returns whether this lane's ray still needs rounds
 // (L then holds its state after its last integrated event, L.lower that event's key).
+//
+// It runs in stages over consecutive t ranges [lo, hi): a stage lists and integrates the
+// leaves the packet can meet in its range; every event below hi is then final, the buffer
+// is dropped, and the next stage starts at hi, taking only events after the last
+// integrated one (L.lower). A range whose lists overflow shared memory is halved and
+// walked again. The first stage covers kFirstStage of the packet's t extent in the scene.
+//
+// Not inlined: one copy per buffer size and SH degree instead of one in every kernel; the
+// ray and its loop state are copied into registers once per packet, the scene and launch
+// constants are read through their references.
 template <int KBUF, int DEG>
-__device__ bool frustum_phase(const SceneRef& sc, const TraceCtx& C, const Ray& ray, const float* B, int bs,
-                              int64_t slot, int* wsm, int lane, bool act, RayLoop& L) {
+__device__ __noinline__ bool frustum_phase(const SceneRef& sc, const TraceCtx& C, const Ray& ray0, const float* B,
+                                           int bs, int64_t slot, int* wsm, int lane, bool act, RayLoop& L0) {
   if (!__any_sync(kFull, act)) return act;
+  const Ray ray = ray0;
+  RayLoop L = L0;
   const RaySlab sl = make_slab(ray);
   const float cap = fminf(C.tmax, kSentinel);
-  const PacketBounds P = packet_bounds(ray, sl, act);
+  PacketBounds P = packet_bounds(ray, sl, act);
+  // the packet's t extent in the scene box (the union of the root's child boxes): no event of
+  // a packet ray lies beyond `end`
+  float end = -INFINITY;
+  {
+    const Node root = load_node(sc.nodes, 0);
+    float tn, tf;
+    if (packet_span(P, root.a.x, root.a.y, root.a.z, root.a.w, root.b.x, root.b.y, 0.f, cap, tn, tf))
+      end = fmaxf(end, tf);
+    if (packet_span(P, root.b.z, root.b.w, root.c.x, root.c.y, root.c.z, root.c.w, 0.f, cap, tn, tf))
+      end = fmaxf(end, tf);
+    end = fminf(end, cap);
+  }
   int* front = wsm + kStackDepth;
   uint64_t* cand = reinterpret_cast<uint64_t*>(front + 2 * kFrontierCap);
-  const int nc = packet_leaves(sc.nodes, P, cap, front, cand, lane);
-  if (nc < 0) return act;  // lists too long for shared memory: the rounds trace the packet
-  sort_keys(cand, nc, lane);
-  uint64_t buf[KBUF];
-#pragma unroll
-  for (int i = 0; i < KBUF; ++i) buf[i] = kEmptyKey;
+  // the bounds wait in shared memory while the leaves are integrated (registers are scarce)
+  PacketBounds* saved = reinterpret_cast<PacketBounds*>(cand + kCandCap);
+  if (lane == 0) *saved = P;
+  __syncwarp();
   bool live = act;  // still integrating in this phase
-  for (int cb = 0;; cb += kLeafGroup) {
-    // every 32 leaves, the lanes start the loads of the next 32 records into L1 (one each),
-    // so the broadcast record loads below rarely wait on L2
-    if ((cb & 31) == 0 && cb + lane < nc)
-      asm volatile("prefetch.global.L1 [%0];" ::"l"(sc.recs + int(uint32_t(cand[cb + lane]))));
-    // events below T are final: no leaf still to come has an event before T. They are
-    // integrated once per group of leaves, when the lanes have several at once.
-    const float T = cb < nc ? key_t(cand[cb]) : INFINITY;
-    while (live && buf[0] != kEmptyKey && key_t(buf[0]) < T) {
-      const uint64_t k = buf[0];
-#pragma unroll
-      for (int i = 0; i < KBUF - 1; ++i) buf[i] = buf[i + 1];
-      buf[KBUF - 1] = kEmptyKey;
-      L.lower = k;
-      if (consume_event<DEG>(sc, C, ray, B, bs, slot, k, L.s, L.last_dirac, L.iters, L.s16, L.cnt16, L.status)) {
-        live = false;
-        act = false;  // finished
-      }
+  float lo = 0.f;
+  float span = kFirstStage * fmaxf(end - lo, 0.f);
+  for (int tries = 0; end >= 0.f && __any_sync(kFull, live);) {
+    const bool last = !(lo + span < end);
+    const float hi = last ? end : lo + span;
+    const int nc = packet_leaves(sc.nodes, *saved, lo, hi, front, cand, lane);
+    if (nc < 0) {  // too many nodes or leaves in this range: halve it
+      if (++tries > kMaxHalvings) break;  // the rounds trace what is left
+      span *= 0.5f;
+      continue;
     }
-    if (cb >= nc) break;
-    if (!__any_sync(kFull, live)) break;
-    // the group's leaves: independent tests (their loads and roots overlap), then inserts
-    uint64_t e0[kLeafGroup], e1[kLeafGroup];
+    sort_keys(cand, nc, lane);
+    uint64_t buf[KBUF];
 #pragma unroll
-    for (int g = 0; g < kLeafGroup; ++g) {
-      e0[g] = e1[g] = kEmptyKey;
-      if (live && cb + g < nc) {
-        const int j = int(uint32_t(cand[cb + g]));
-        HitT H;
-        if (intersect(load_record(sc.recs, j), ray, H)) {
-          const bool in0 = H.t0 > L.s16 && H.t0 <= C.tmax;
-          if (in0) e0[g] = event_key(H.t0, j, 0);
-          if (H.t1 > L.s16 && (H.t1 <= C.tmax || in0)) e1[g] = event_key(H.t1, j, 1);
+    for (int i = 0; i < KBUF; ++i) buf[i] = kEmptyKey;
+    const float t_final = last ? INFINITY : hi;
+    for (int cb = 0;; cb += kLeafGroup) {
+      // every 32 leaves, the lanes start the loads of the next 32 records into L1 (one
+      // each), so the broadcast record loads below rarely wait on L2
+      if ((cb & 31) == 0 && cb + lane < nc)
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(sc.recs + int(uint32_t(cand[cb + lane]))));
+      // events below T are final: no leaf still to come has an event before T. They are
+      // integrated once per group of leaves, when the lanes have several at once.
+      const float T = cb < nc ? key_t(cand[cb]) : t_final;
+      while (live && buf[0] != kEmptyKey && key_t(buf[0]) < T) {
+        const uint64_t k = buf[0];
+#pragma unroll
+        for (int i = 0; i < KBUF - 1; ++i) buf[i] = buf[i + 1];
+        buf[KBUF - 1] = kEmptyKey;
+        L.lower = k;
+        if (consume_event<DEG>(sc, C, ray, B, bs, slot, k, L.s, L.last_dirac, L.iters, L.s16, L.cnt16, L.status)) {
+          live = false;
+          act = false;  // finished
+        }
+      }
+      if (cb >= nc) break;
+      if (!__any_sync(kFull, live)) break;
+      // the group's leaves: independent tests (their loads and roots overlap), then inserts
+      uint64_t e0[kLeafGroup], e1[kLeafGroup];
+#pragma unroll
+      for (int g = 0; g < kLeafGroup; ++g) {
+        e0[g] = e1[g] = kEmptyKey;
+        if (live && cb + g < nc) {
+          const int j = int(uint32_t(cand[cb + g]));
+          HitT H;
+          if (intersect(load_record(sc.recs, j), ray, H)) {
+            const bool in0 = H.t0 > L.s16 && H.t0 <= C.tmax;
+            if (in0) e0[g] = event_key(H.t0, j, 0);
+            if (H.t1 > L.s16 && (H.t1 <= C.tmax || in0)) e1[g] = event_key(H.t1, j, 1);
+          }
+        }
+      }
+#pragma unroll
+      for (int g = 0; g < kLeafGroup; ++g) {
+#pragma unroll
+        for (int x = 0; x < 2; ++x) {
+          const uint64_t e = x ? e1[g] : e0[g];
+          // earlier stages integrated everything up to L.lower
+          if (live && e != kEmptyKey && e > L.lower) {
+            // a full buffer cannot take another event: stop here, the rounds continue the ray
+            if (buf[KBUF - 1] != kEmptyKey) live = false;
+            else buf_insert(buf, e);
+          }
         }
       }
     }
-#pragma unroll
-    for (int g = 0; g < kLeafGroup; ++g) {
-#pragma unroll
-      for (int x = 0; x < 2; ++x) {
-        const uint64_t e = x ? e1[g] : e0[g];
-        if (live && e != kEmptyKey) {
-          // a full buffer cannot take another event: stop here, the rounds continue the ray
-          if (buf[KBUF - 1] != kEmptyKey) live = false;
-          else buf_insert(buf, e);
-        }
-      }
+    if (last) {
+      // every stage done and every event integrated: nothing is left on a lane still active
+      if (live) act = false;
+      break;
     }
+    lo = hi;
+    span = end - lo;
+    tries = 0;
   }
-  // all leaves taken and every event integrated: nothing is left on a lane still active
-  if (live) act = false;
+  if (end < 0.f) act = false;  // the packet misses the scene: no events at all
+  L0 = L;
   return act;
 }
 
