@@ -35,7 +35,7 @@ class EverBackwardOut(ctypes.Structure):
 
 
 class EverTraceArgs(ctypes.Structure):
-    _fields_ = [("tmin", c_f32), ("tmax", c_f32), ("max_iters", c_i32), ("sh_degree", c_i32)]
+    _fields_ = [("tmin", c_f32), ("tmax", c_f32), ("max_iters", c_i32), ("sh_degree", c_i32), ("depth_hint", c_p)]
 
 
 class EverBatchView(ctypes.Structure):

@@ -130,6 +130,7 @@ int ever_trace_forward(const EverScene* scene, const float* rayo, const float* r
   P.max_iters = args->max_iters;
   P.ray_order = ray_order;
   P.out = *out;
+  P.depth_hint = args->depth_hint;
   return cuda_status(ever::launch_forward(P, deg, resolve_tune(tune), static_cast<cudaStream_t>(stream)),
                      "ever_trace_forward");
 }
@@ -168,6 +169,7 @@ int ever_trace_forward_regrouped(const EverScene* scene, const float* rayo, cons
   P.max_iters = args->max_iters;
   P.ray_order = ray_order;
   P.out = *out;
+  P.depth_hint = args->depth_hint;
   if (num_rays == 0) return EVER_OK;
   const ever::RegroupScratch W = ever::regroup_scratch(static_cast<char*>(workspace), num_rays);
   return cuda_status(ever::launch_forward_regrouped(P, W, nullptr, nullptr, deg, resolve_tune(tune),
@@ -395,6 +397,7 @@ int ever_trace_forward_camera(const EverScene* scene, const EverCamera* camera, 
   P.tmax = args->tmax;
   P.max_iters = args->max_iters;
   P.out = *out;
+  P.depth_hint = args->depth_hint;
   return cuda_status(
       ever::launch_forward_camera(P, C, jitter, deg, resolve_tune(tune), static_cast<cudaStream_t>(stream)),
       "ever_trace_forward_camera");
@@ -429,6 +432,7 @@ int ever_trace_forward_camera_regrouped(const EverScene* scene, const EverCamera
   P.tmax = args->tmax;
   P.max_iters = args->max_iters;
   P.out = *out;
+  P.depth_hint = args->depth_hint;
   if (R == 0) return EVER_OK;
   const ever::RegroupScratch W = ever::regroup_scratch(static_cast<char*>(workspace), S);
   return cuda_status(ever::launch_forward_regrouped(P, W, &C, jitter, deg, resolve_tune(tune),

@@ -72,6 +72,7 @@ struct FwdParams {
   EverForwardOut out;
   int frustum;  // packet kernels: frustum phase before the rounds (set from the tune)
   int stack_depth;  // traversal stack entries in use, <= kStackDepth (set from the tune)
+  const float* depth_hint;  // (R) nullable: per-ray guess of the stopping t (first frustum stage)
 };
 
 cudaError_t launch_forward(const FwdParams& P, int deg, const EverTune& tune, cudaStream_t st);

@@ -296,6 +296,7 @@ struct TraceCtx {
   EverForwardOut out;
   bool frustum;        // packet kernels: run the frustum phase before the rounds
   int depth;           // traversal stack entries in use (<= kStackDepth)
+  const float* depth_hint;  // (R) nullable: per-ray guess of the stopping t
 };
 
 // One event of a ray's sorted sequence, integrated under the reference's round rules
@@ -425,7 +426,7 @@ __global__ void __launch_bounds__(256) k_trace_fwd_ray(const FwdParams P) {
   if (gi >= P.R) return;
   const int64_t r = P.ray_order ? int64_t(P.ray_order[gi]) : gi;
   const SceneRef sc = scene_of(P);
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out, P.frustum != 0, P.stack_depth};
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out, P.frustum != 0, P.stack_depth, P.depth_hint};
   const Ray ray = load_ray(P.rayo, P.rayd, r, P.tmin);
   const RaySlab sl = make_slab(ray);
   float B[16];
@@ -770,7 +771,8 @@ __device__ __forceinline__ void sort_keys(uint64_t* cand, int n, int lane) {
 // constants are read through their references.
 template <int KBUF, int DEG>
 __device__ __noinline__ bool frustum_phase(const SceneRef& sc, const TraceCtx& C, const Ray& ray0, const float* B,
-                                           int bs, int64_t slot, int* wsm, int lane, bool act, RayLoop& L0) {
+                                           int bs, int64_t slot, int64_t r, int* wsm, int lane, bool act,
+                                           RayLoop& L0) {
   if (!__any_sync(kFull, act)) return act;
   const Ray ray = ray0;
   RayLoop L = L0;
@@ -798,6 +800,12 @@ __device__ __noinline__ bool frustum_phase(const SceneRef& sc, const TraceCtx& C
   bool live = act;  // still integrating in this phase
   float lo = 0.f;
   float span = kFirstStage * fmaxf(end - lo, 0.f);
+  if (C.depth_hint) {
+    // the first stage reaches the packet's largest guessed stopping t (plus 5%); a ray that
+    // goes on continues in the next stage, so a poor guess costs time, never correctness
+    const float h = warp_max(act ? C.depth_hint[r] : -INFINITY);
+    if (h > 0.f && h < INFINITY) span = fminf(span, 1.05f * h + 1e-3f);
+  }
   for (int tries = 0; end >= 0.f && __any_sync(kFull, live);) {
     const bool last = !(lo + span < end);
     const float hi = last ? end : lo + span;
@@ -884,7 +892,7 @@ __device__ __forceinline__ void trace_packet(const SceneRef& sc, const TraceCtx&
   store_basis<DEG>(ray, B, bs);
   RayLoop L = start_ray<DEG>(sc, ray, valid, wstack, C.depth, B, bs, lane);
   bool act = valid && C.max_iters > 0 && sc.N > 0;
-  if (C.frustum) act = frustum_phase<KBUF, DEG>(sc, C, ray, B, bs, slot, wstack, lane, act, L);
+  if (C.frustum) act = frustum_phase<KBUF, DEG>(sc, C, ray, B, bs, slot, r, wstack, lane, act, L);
   run_rounds<KBUF, DEG>(sc, C, ray, B, bs, slot, wstack, lane, act, L, INT_MAX);
   if (valid) write_outputs(C.out, r, L.s, L.last_dirac, L.iters, L.status);
   __syncwarp();
@@ -942,7 +950,7 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value) k_trace_fwd
   const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;
   const bool valid = gi < P.R;  // every lane stays for the warp-wide ballots
   const int64_t r = valid ? (P.ray_order ? int64_t(P.ray_order[gi]) : gi) : 0;
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out, P.frustum != 0, P.stack_depth};
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out, P.frustum != 0, P.stack_depth, P.depth_hint};
   const Ray ray = load_ray(P.rayo, P.rayd, r, P.tmin);
   trace_packet<KBUF, DEG>(scene_of(P), C, ray, r, valid, gi, wstack, B, blockDim.x, lane);
 }
@@ -986,7 +994,7 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value)
   }
   if (!valid) r = 0;
   const SceneRef sc = scene_of(P);
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, slots, P.out, P.frustum != 0, P.stack_depth};
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, slots, P.out, P.frustum != 0, P.stack_depth, P.depth_hint};
   Ray ray;
   if (CAM) {
     float3 ro, rd;
@@ -1001,7 +1009,7 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value)
   if (PASS == 0) {
     L = start_ray<DEG>(sc, ray, valid, wstack, C.depth, B, blockDim.x, lane);
     act = valid && C.max_iters > 0 && sc.N > 0;
-    if (C.frustum) act = frustum_phase<KBUF, DEG>(sc, C, ray, B, blockDim.x, slot, wstack, lane, act, L);
+    if (C.frustum) act = frustum_phase<KBUF, DEG>(sc, C, ray, B, blockDim.x, slot, r, wstack, lane, act, L);
   } else {
     if (valid) L = resume_ray(P.out, r);
     act = valid;
@@ -1036,7 +1044,7 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value)
   const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;
   const int64_t p = gi < num_slots ? camera_slot_pixel(cam, gi) : -1;
   const bool valid = p >= 0;
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, num_slots, P.out, P.frustum != 0, P.stack_depth};
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, num_slots, P.out, P.frustum != 0, P.stack_depth, P.depth_hint};
   float3 ro, rd;
   camera_ray(cam, jitter, valid ? p : 0, ro, rd);
   const Ray ray = make_ray(ro, rd, P.tmin);
@@ -1051,7 +1059,7 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value) k_trace_fwd
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   int* wstack = smem + warp * kWarpInts;  // stack, then the frustum phase's lists
   float* B = reinterpret_cast<float*>(smem + (blockDim.x / 32) * kWarpInts) + tid;
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.num_slots, P.out, P.frustum != 0, P.stack_depth};
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.num_slots, P.out, P.frustum != 0, P.stack_depth, nullptr};
   const int64_t num_packets = P.num_slots / 32;
   for (;;) {
     unsigned int pk = 0;

@@ -171,6 +171,20 @@ def cost_targets(ray_stats: torch.Tensor, rayo: torch.Tensor, rayd: torch.Tensor
     return t
 
 
+def depth_from_prediction(pred: torch.Tensor, rayo: torch.Tensor, rayd: torch.Tensor, centre=(0.0, 0.0, 0.0),
+                          scale: float = 1.0, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """(R,) stopping t guessed by the model (the inverse of cost_targets' depth column): the
+    depth hint the tracer's frustum phase takes (tracer.forward(depth_hint=...))."""
+    c = torch.tensor(centre, dtype=torch.float32, device=rayo.device)
+    n = rayd.norm(dim=1).clamp_min(1e-30)
+    s_c = -((rayo - c) * rayd).sum(1) / n
+    d = (pred[:, 1] * scale + s_c) / n
+    if out is None:
+        return d
+    out.copy_(d)
+    return out
+
+
 def quantile_thresholds(pred_cost: torch.Tensor, qs=(0.25, 0.5, 0.75), max_samples=1 << 22):
     """Three thresholds at quantiles of predicted log-costs (from the training rays)."""
     x = pred_cost.flatten().float()

@@ -127,18 +127,21 @@ class ForwardResult:
     status: torch.Tensor          # (1,) int32
 
 
-def trace_args(tmin, tmax, max_iters, sh_degree):
-    """sh_degree None: the reference's DC-only forward colour; d: SH of degree d along rayd."""
+def trace_args(tmin, tmax, max_iters, sh_degree, depth_hint=None):
+    """sh_degree None: the reference's DC-only forward colour; d: SH of degree d along rayd.
+    depth_hint: optional (R,) float32 device tensor, a guess per ray of the t at which it stops
+    (the frustum phase's first stage covers up to a packet's largest guess)."""
     a = N.EverTraceArgs()
     a.tmin, a.tmax, a.max_iters = float(tmin), float(tmax), int(max_iters)
     a.sh_degree = -1 if sh_degree is None else int(sh_degree)
+    a.depth_hint = N.ptr(depth_hint)
     return a
 
 
 def forward(scene: Scene, rayo, rayd, tmin=0.0, tmax=1000.0, max_iters=500, sh_degree=None, log_events=True,
             touch_count=False, ray_stats=False, ray_order=None, tune: Tune | None = None,
             buffers: ForwardResult | None = None, regrouped: bool = True,
-            workspace: torch.Tensor | None = None) -> ForwardResult:
+            workspace: torch.Tensor | None = None, depth_hint: torch.Tensor | None = None) -> ForwardResult:
     """regrouped: with warp packets (tune.traversal 0) and k-buffers of up to 16 events,
     re-pack the rays that need more gather rounds into full warps between passes
     (ever_trace_forward_regrouped; same results, faster). workspace: optional uint8 scratch
@@ -171,7 +174,12 @@ def forward(scene: Scene, rayo, rayd, tmin=0.0, tmax=1000.0, max_iters=500, sh_d
     o.touch_count = N.ptr(buffers.touch_count)
     o.ray_stats = N.ptr(buffers.ray_stats)
     o.status = N.ptr(buffers.status)
-    args = trace_args(tmin, tmax, max_iters, sh_degree)
+    if depth_hint is not None:
+        _check_tensor("depth_hint", depth_hint, device)
+        if depth_hint.numel() != R:
+            raise RuntimeError("depth_hint must hold one value per ray")
+        depth_hint = depth_hint.contiguous()
+    args = trace_args(tmin, tmax, max_iters, sh_degree, depth_hint)
     tune = tune or Tune()
     lib = N.load()
     with torch.cuda.device(device):

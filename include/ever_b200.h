@@ -106,6 +106,10 @@ typedef struct EverTraceArgs {
                          the ellipsoid's DC term C0*f0 + 0.5 whatever K (shaders.slang:72-75,
                          eval_sh_col0), and its gradient in the backward (features k >= 1 get
                          zero); 0..3: SH of that degree along the raw rayd in both passes */
+  const float* depth_hint; /* (R) device, nullable: a guess per ray of the t at which it stops (e.g.
+                              the ray-cost model's). A packet's first frustum stage then covers the
+                              t range up to its largest guess instead of the whole scene; rays that
+                              go on continue in the next stage. Results do not depend on it. */
 } EverTraceArgs;
 
 const char* ever_last_error(void);

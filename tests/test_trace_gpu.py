@@ -167,6 +167,26 @@ def test_nested_shells_overflow_the_pending_buffer_midway():
     assert torch.equal(fwd.out, ref.out) and torch.equal(fwd.states, ref.states) and np.array_equal(tri, tref)
 
 
+@pytest.mark.parametrize("kind", ["half", "true", "random", "zero"])
+def test_depth_hint_changes_no_result(kind):
+    # the hint only sets where a packet's first frustum stage ends: rays that go on continue
+    # in later stages, so any hint, good or bad, gives the same bits
+    dev = _dev()
+    sc = S.clustered_scene(30_000, 0, seed=51, n_clusters=60)
+    ro, rd = S.look_at_rays(S.Camera(S.sphere_point(4.0, 51), 64, 48, 50.0))
+    scene, ref, tref = _gpu_trace(sc, ro, rd)
+    depth = ref.ray_stats[:, 1].clone()
+    hint = {"half": 0.5 * depth, "true": depth, "zero": torch.zeros_like(depth),
+            "random": torch.rand(depth.shape, device=dev, generator=torch.Generator(device=dev).manual_seed(5)) * 8}[kind]
+    t = lambda a: torch.tensor(np.ascontiguousarray(a, np.float32), device=dev)
+    got = T.forward(scene, t(ro), t(rd), log_events=True, ray_stats=True, depth_hint=hint.contiguous())
+    tri = T.reference_tri_collection(scene, got, 500).cpu().numpy().reshape(500, -1)
+    for k in ("out", "states", "iters", "last_dirac"):
+        assert torch.equal(getattr(got, k), getattr(ref, k)), k
+    assert np.array_equal(tri, tref)
+    assert int(got.status.item()) == 0
+
+
 def test_duplicate_ellipsoids_round_boundary():
     # 20 identical ellipsoids: ties at the reference's 16-event round boundary
     N = 20
