@@ -377,16 +377,20 @@ def leg_batched(dev, reps=3):
 
 
 def leg_sched(dev, test_views=56):
-    """Learned ray-cost scheduler on a 64-view orbit of 3M clustered ellipsoids: the MLP is
-    trained on the first 8 views' per-ray logs, then the remaining views are traced forward
-    + backward in plain order, coherent order, learned cost-binned order (MLP inference and
-    sort inside the timed region), the learned order in batched persistent launches of 8
-    views, and cost bins from the true logged costs (a ceiling no predictor can beat)."""
+    """Learned ray-cost model on a 64-view orbit of 3M clustered ellipsoids: the MLP is
+    trained on the first 8 views' per-ray logs (events consumed, stopping depth), then the
+    remaining views are traced forward + backward with
+    - plain: ray-index launch order;
+    - coherent: the direction-sorted launch order (ever_ray_order);
+    - learned_bins: predicted cost bins, costliest first, coherent inside each bin;
+    - learned_depth: coherent order, and the predicted stopping depth as the frustum phase's
+      depth hint (MLP inference inside the timed region);
+    - true_depth: the same with the logged stopping depth, the ceiling no predictor passes.
+    Every image is compared bit for bit with the plain order's."""
     import torch
     from ever_b200 import scheduler as SCH
     from ever_b200 import synthetic as S
     from ever_b200 import tracer as T
-    from ever_b200.batched import BatchedTracer
     n_train, W, H = 8, 1920, 1080
     sc, cams = S.workload_orbit(n=3_000_000, n_views=64, width=W, height=H)
     arrs = tuple(torch.tensor(np.ascontiguousarray(a), device=dev) for a in
@@ -412,41 +416,47 @@ def leg_sched(dev, test_views=56):
     cm.check()
     losses = losses[0].cpu().numpy()
     thr = SCH.quantile_thresholds(cm.predict(ro_tr, rd_tr)[0][:, 0])
-    true_thr = SCH.quantile_thresholds(torch.log1p(st_tr[:, 0]))
     del ro_tr, rd_tr, st_tr, tg
     test = list(range(n_train, n_train + test_views))
     pred_buf = torch.empty((R, 2), device=dev)
     bins_buf = torch.empty(R, dtype=torch.uint8, device=dev)
     order_buf = torch.empty(R, dtype=torch.int32, device=dev)
+    hint_buf = torch.empty(R, device=dev)
     predict_ms = _timed(lambda: cm.predict(*rays[test[0]], thresholds=thr, out=pred_buf, bins_out=bins_buf), dev)
-    r2 = []
-    true_bins = {}
+    r2_events, r2_depth = [], []
+    true_depth = {}
     for v in test:
-        p, _ = cm.predict(*rays[v])
-        t = torch.log1p(stats[v][:, 0])
-        r2.append(1 - float(((p[:, 0] - t) ** 2).mean() / t.var()))
-        true_bins[v] = ((t > true_thr[0]).int() + (t > true_thr[1]).int() + (t > true_thr[2]).int()).to(torch.uint8)
+        ro, rd = rays[v]
+        p, _ = cm.predict(ro, rd)
+        t = SCH.cost_targets(stats[v], ro, rd, scale=2.0)
+        r2_events.append(1 - float(((p[:, 0] - t[:, 0]) ** 2).mean() / t[:, 0].var()))
+        r2_depth.append(1 - float(((p[:, 1] - t[:, 1]) ** 2).mean() / t[:, 1].var()))
+        true_depth[v] = stats[v][:, 1].clone()
     del stats
     gout = torch.full((R, 5), 0.1, device=dev)
     fbuf = [None]
     bws = [None]
     outs = {}
 
-    def order_of(kind, v):
+    def plan(kind, v):
         ro, rd = rays[v]
         if kind == "plain":
-            return None
-        if kind == "coherent":
-            return T.ray_order(ro, rd, ws)
-        if kind == "learned":
+            return None, None
+        if kind == "learned_bins":
             cm.predict(ro, rd, thresholds=thr, out=pred_buf, bins_out=bins_buf)
-            return SCH.binned_order(ro, rd, bins_buf, ws, order_buf)
-        return SCH.binned_order(ro, rd, true_bins[v], ws, order_buf)
+            return SCH.binned_order(ro, rd, bins_buf, ws, order_buf), None
+        order = T.ray_order(ro, rd, ws)
+        if kind == "learned_depth":
+            cm.predict(ro, rd, out=pred_buf)
+            return order, SCH.depth_from_prediction(pred_buf, ro, rd, scale=2.0, out=hint_buf)
+        if kind == "true_depth":
+            return order, true_depth[v]
+        return order, None
 
     def one(kind, v):
         ro, rd = rays[v]
-        o = order_of(kind, v)
-        f = T.forward(scene, ro, rd, 0.0, 1000.0, 500, ray_order=o, buffers=fbuf[0])
+        o, hint = plan(kind, v)
+        f = T.forward(scene, ro, rd, 0.0, 1000.0, 500, ray_order=o, buffers=fbuf[0], depth_hint=hint)
         fbuf[0] = f
         slots = T.backward_order(f, o, 0, ws)  # as trace_rays' backward: replay grouped by event count
         g = T.backward(scene, ro, rd, f, gout, 0.0, 1000.0, 500, ray_order=o, workspace=bws[0], slot_order=slots)
@@ -456,7 +466,7 @@ def leg_sched(dev, test_views=56):
     bws[0] = torch.empty(int(T.N.load().ever_backward_workspace_bytes(scene.num_prims, scene.sh_coeffs)),
                          dtype=torch.uint8, device=dev)
     identical = True
-    kinds = ("plain", "coherent", "learned", "true")
+    kinds = ("plain", "coherent", "learned_bins", "learned_depth", "true_depth")
     for kind in kinds:
         one(kind, test[0])
         for v in test:  # images of every order against the plain order's
@@ -474,17 +484,6 @@ def leg_sched(dev, test_views=56):
     ms = {kind: float(np.median(reps[kind])) for kind in kinds}
     del fbuf[0], bws[0]
     torch.cuda.empty_cache()
-    # learned order in batched persistent launches (8 views per launch; graph capture)
-    batched_ms = 0.0
-    for i in range(0, len(test), 8):
-        grp = test[i:i + 8]
-        bt = BatchedTracer([arrs], [(0, *rays[v]) for v in grp], max_iters=500, graph=True, scheduler=(cm, thr))
-        g = torch.full((bt.R, 5), 0.1, device=dev)
-        batched_ms += _timed(lambda: bt.step(g), dev)
-        for j, v in enumerate(grp):
-            identical &= bool(torch.equal(bt.out[bt.view_slice(j)], outs[v]))
-        del bt, g
-        torch.cuda.empty_cache()
     rays_total = R * len(test)
     mr = lambda t: rays_total / (t * 1e-3) / 1e6
     flop_per_ray = 2 * (39 * 64 + 64 * 64 + 64 * 2)
@@ -497,16 +496,13 @@ def leg_sched(dev, test_views=56):
     return {
         "workload": f"3M clustered ellipsoids SH3, 64-view orbit at radius 4, {W}x{H}; MLP trained on views 0-7, "
                     f"views 8-{7 + test_views} traced forward + backward",
-        "mrays_fwdbwd": {"plain": mr(ms["plain"]), "coherent": mr(ms["coherent"]), "learned": mr(ms["learned"]),
-                         "learned_batched": mr(batched_ms), "true_cost_bins": mr(ms["true"])},
-        "ms_total": dict(ms, learned_batched=batched_ms),
+        "mrays_fwdbwd": {k: mr(ms[k]) for k in kinds},
+        "ms_total": ms,
         "ms_passes": reps,
-        "speedup_learned_vs_plain": ms["plain"] / ms["learned"],
-        "speedup_learned_batched_vs_plain": ms["plain"] / batched_ms,
-        "speedup_learned_vs_coherent": ms["coherent"] / ms["learned"],
-        "speedup_true_cost_bins_vs_coherent": ms["coherent"] / ms["true"],
+        "speedup_vs_plain": {k: ms["plain"] / ms[k] for k in kinds},
+        "speedup_vs_coherent": {k: ms["coherent"] / ms[k] for k in kinds},
         "images_bit_identical_to_plain": identical,
-        "heldout_r2_log_events_mean": float(np.mean(r2)),
+        "heldout_r2": {"log_events": float(np.mean(r2_events)), "depth": float(np.mean(r2_depth))},
         "train": {"samples": R * n_train, "steps": int(len(losses)), "fit_ms": fit_ms,
                   "loss_first": float(losses[0]), "loss_last": float(losses[-1])},
         "mlp_predict": {"ms_per_view": predict_ms, "rays": R, "tflops": mlp_tflops, "peak_tflops": bf16_peak,
@@ -737,7 +733,8 @@ def main():
         line["batched"] = leg_batched(dev)
     if rank == 0 and world == 1 and not args.no_sched:
         line["sched"] = leg_sched(dev, args.sched_views)
-        line["learned_sched_vs_plain_speedup"] = line["sched"]["speedup_learned_vs_plain"]
+        line["learned_sched_vs_plain_speedup"] = line["sched"]["speedup_vs_plain"]["learned_depth"]
+        line["learned_sched_vs_coherent_speedup"] = line["sched"]["speedup_vs_coherent"]["learned_depth"]
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -540,6 +540,7 @@ constexpr int kCandCap = 512;      // leaves per packet (a power of two: the sor
 constexpr int kLeafGroup = 4;      // leaves tested together before their events are inserted
 constexpr float kFirstStage = 1.0f;  // the first stage's share of the packet's t extent
 constexpr int kMaxHalvings = 24;     // halvings of an overflowing range before the rounds take over
+constexpr int kMaxWalks = 64;        // breadth-first walks per packet before the rounds take over
 // Shared ints per warp: the traversal stack, two frontier levels, the leaf keys (64-bit),
 // the packet's bounds between stages.
 constexpr int kBoundsInts = 20;
@@ -806,9 +807,14 @@ __device__ __noinline__ bool frustum_phase(const SceneRef& sc, const TraceCtx& C
     const float h = warp_max(act ? C.depth_hint[r] : -INFINITY);
     if (h > 0.f && h < INFINITY) span = fminf(span, 1.05f * h + 1e-3f);
   }
+  int walks = 0;
   for (int tries = 0; end >= 0.f && __any_sync(kFull, live);) {
+    // bounded: at most kMaxWalks walks, and every stage must advance lo in float;
+    // otherwise the rounds trace what is left
+    if (++walks > kMaxWalks) break;
     const bool last = !(lo + span < end);
     const float hi = last ? end : lo + span;
+    if (!last && !(hi > lo)) break;
     const int nc = packet_leaves(sc.nodes, *saved, lo, hi, front, cand, lane);
     if (nc < 0) {  // too many nodes or leaves in this range: halve it
       if (++tries > kMaxHalvings) break;  // the rounds trace what is left
@@ -876,7 +882,7 @@ __device__ __noinline__ bool frustum_phase(const SceneRef& sc, const TraceCtx& C
       break;
     }
     lo = hi;
-    span = end - lo;
+    span = fminf(2.f * span, end - lo);  // the next range may be wider again
     tries = 0;
   }
   if (end < 0.f) act = false;  // the packet misses the scene: no events at all
