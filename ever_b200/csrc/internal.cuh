@@ -234,7 +234,6 @@ cudaError_t launch_log_to_reference(const int32_t* order, const int32_t* log, in
 constexpr int kOffW1 = 0, kOffW2 = 4096, kOffW3 = 8192, kOffB1 = 9216, kOffB2 = 9280, kOffB3 = 9344;
 constexpr int kMlpParams = 9360;
 constexpr int kMlpMaxGrid = 160;  // CTAs of a gradient launch (one partial-gradient slot each)
-constexpr int kMlpInferCtasPerSm = 6;  // resident inference CTAs per SM (64 TMEM columns each)
 
 struct MlpParams {
   const void* w1;  // bf16 [64 x 64]
@@ -259,8 +258,9 @@ struct MlpParams {
   long long wait_clocks;  // bound of each tensor-core completion wait (0: about a second)
 };
 
-cudaError_t launch_mlp(const MlpParams& P, bool train, int max_grid, cudaStream_t st);
-int mlp_grid(int64_t num_samples, int max_grid);  // CTAs launch_mlp uses
+// One persistent CTA per SM at most; `grid` from mlp_grid.
+cudaError_t launch_mlp(const MlpParams& P, bool train, int grid, cudaStream_t st);
+int mlp_grid(int64_t num_samples, int max_grid, bool train);
 cudaError_t launch_mlp_reduce(const float* partial, int grid, float* grads, float* loss, cudaStream_t st);
 cudaError_t launch_mlp_adam(float* params, const float* grads, float* m, float* v, void* w1, void* w2, void* w3,
                             float lr, float beta1, float beta2, float eps, int step, cudaStream_t st);

@@ -4,16 +4,25 @@
 //
 // Input encoding of a ray (o, d): p = (o - c) - ((o - c).d^) d^, the point of the ray's
 // line closest to the scene centre c, times 1/scale; then x, sin(2^k pi x), cos(2^k pi x)
-// for k = 0..5 per component: 3 + 36 = 39 features, zero-padded to 64 columns. Outputs:
+// for k = 0..5 per component: 3 + 36 = 39 features, zero-padded to 48 columns (the first
+// layer's K; the parameter block keeps W1 64 wide, its columns 39.. are padding). Outputs:
 // the cost the tracer logs per ray, [log(1 + consumed events), depth offset / scale].
 //
-// One CTA of 128 threads (one warpgroup) loops over tiles of 128 rays (the MMA's M).
+// One persistent CTA per SM, warp-specialised:
+// - kWorkers worker warpgroups. Each takes its own tiles of 128 rays (the MMA's M): it
+//   encodes a tile into shared memory, and after each layer's MMAs reads the accumulator
+//   from tensor memory (bias, ReLU, bf16) into the next layer's operand tile. The rays of
+//   its next tile are loaded into registers while the current tile's MMAs run.
+// - one MMA warp. One thread issues every tcgen05.mma of the CTA: it serves the workers'
+//   requests in a fixed round-robin order, each request one layer (or one backward step)
+//   of one tile, and tcgen05.commit signals that worker's completion barrier.
+// The workers' CUDA-core work (encoding, epilogues) overlaps the other workers' MMAs.
 // Operands live in shared memory in the canonical no-swizzle layouts: 8 x 8 bf16 core
 // matrices of 128 contiguous bytes. Activation tiles [ray][unit] are K-major operands of
 // the layer products; the same bytes are the MN-major operands of the weight-gradient
-// products, which reduce over rays. Thread 0 issues the MMAs and tcgen05.commit signals
-// their completion on an mbarrier; every wait is bounded and reports a timeout through an
-// error flag instead of hanging.
+// products, which reduce over rays. Training accumulates the weight and bias gradients of
+// all the CTA's tiles in tensor memory; the fixed service order makes the sums
+// deterministic. Every wait is bounded and reports a timeout through an error flag.
 #include <cstddef>
 
 #include <cuda_bf16.h>
@@ -25,16 +34,20 @@ namespace ever {
 namespace {
 
 constexpr int kTile = 128;  // rays per tile = MMA M
-constexpr int kIn = 64;     // padded encoding width
+constexpr int kK0 = 48;     // encoding columns the first layer reads (39 used)
+constexpr int kFeat = 39;
+constexpr int kIn = 64;     // row length of W1 in the parameter block
 constexpr int kHid = 64;
 constexpr int kOut = 16;    // padded output width (2 used)
-// tensor-memory columns: layer accumulators, then (training) weight-gradient accumulators
-constexpr uint32_t kColD1 = 0, kColD2 = 64, kColD3 = 128, kColGW1 = 256, kColGW2 = 320, kColGW3 = 384;
-// inference: every layer's accumulator reuses D1's columns (each is read out before the next
-// MMA is issued), and one activation tile serves all three layers
-constexpr uint32_t kColsInfer = 64, kColsTrain = 512;
-constexpr size_t kTrainSmem = 120 * 1024;  // keeps one training CTA (512 TMEM columns) per SM
-constexpr int kInferCtasPerSm = kMlpInferCtasPerSm;  // 6 x 64 TMEM columns, about 37 KB shared memory each
+constexpr int kOnes = 16;   // columns of the all-ones operand of the bias-gradient products
+constexpr int kWorkers = 4;
+constexpr int kMmaWarp = 4 * kWorkers;
+constexpr int kThreads = 32 * (kMmaWarp + 1);
+// tensor-memory columns: worker w's layer accumulator at 64 w; training adds the
+// weight- and bias-gradient accumulators (M = 64)
+constexpr uint32_t kColGW1 = 256, kColGW2 = 320, kColGW3 = 384, kColGB1 = 400, kColGB2 = 416;
+constexpr uint32_t kColsInfer = 256, kColsTrain = 512;
+constexpr int kInferSteps = 3, kTrainSteps = 6;  // MMA requests per tile
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -101,6 +114,29 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t phase) {
       : "memory");
   return ok != 0;
 }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// Barrier among the 128 threads of one worker warpgroup (ids 1.. ; 0 is __syncthreads).
+__device__ __forceinline__ void worker_sync(int w) {
+  asm volatile("bar.sync %0, 128;" ::"r"(w + 1) : "memory");
+}
+
+// True on every thread of worker w iff `v` holds on all of them (a barrier with an AND
+// reduction), so the warpgroup leaves its loop together.
+__device__ __forceinline__ bool worker_and(int w, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.and.pred p, %2, 128, q;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(r)
+      : "r"(uint32_t(v)), "r"(w + 1)
+      : "memory");
+  return r != 0;
+}
 
 constexpr long long kWaitClocks = 1ll << 31;  // about a second
 // Bounded wait for phase `phase` of the barrier; false once `limit` clocks have passed.
@@ -118,8 +154,19 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, long lo
   return true;
 }
 
-// 16 consecutive fp32 columns of this thread's TMEM lane.
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+// Consecutive fp32 columns of this thread's TMEM lane.
+template <int N>
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, float (&v)[N]);
+template <>
+__device__ __forceinline__ void tmem_ld<2>(uint32_t taddr, float (&v)[2]) {
+  uint32_t r[2];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0,%1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+  v[0] = __uint_as_float(r[0]);
+  v[1] = __uint_as_float(r[1]);
+}
+template <>
+__device__ __forceinline__ void tmem_ld<16>(uint32_t taddr, float (&v)[16]) {
   uint32_t r[16];
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
@@ -130,36 +177,49 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
+template <>
+__device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
 
-struct Smem {
-  float b1[kHid], b2[kHid], b3[kOut];
-  float gb1[4][kHid], gb2[4][kHid], gb3[4][kOut], loss[4];  // per-warp sums (fixed order)
-  uint64_t bar;
-  uint32_t tmem_base;
-  __align__(128) __nv_bfloat16 w1[kHid * kIn];  // [h1][in]  K-major, rows = output units
-  __nv_bfloat16 w2[kHid * kHid];                 // [h2][h1]
-  __nv_bfloat16 w3[kOut * kHid];                 // [out][h2]
-  __nv_bfloat16 a0[kTile * kIn];                 // encoding (inference: also hidden 1 and 2) [ray][in]
-  // training only: inference launches with the shared memory up to here
-  __nv_bfloat16 a1[kTile * kHid];  // hidden 1            [ray][h1]
-  __nv_bfloat16 a2[kTile * kHid];  // hidden 2            [ray][h2]
-  __nv_bfloat16 g3[kTile * kOut];  // dL/d output         [ray][out]
-  __nv_bfloat16 g2[kTile * kHid];  // dL/d pre-act 2      [ray][h2]
-  __nv_bfloat16 g1[kTile * kHid];  // dL/d pre-act 1      [ray][h1]
-};
-
+// bf16(relu(a + b)) of two columns, packed (column 2j in the low half): one paired fp32
+// add (each lane rounds as a scalar add) and one converting, clamping cvt. ReLU before
+// or after the rounding gives the same bf16 value.
+__device__ __forceinline__ uint32_t bias_relu_bf16x2(float a0, float a1, float b0, float b1) {
+  uint64_t x, y, z;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(x) : "f"(a0), "f"(a1));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(y) : "f"(b0), "f"(b1));
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(z) : "l"(x), "l"(y));
+  float lo, hi;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(z));
+  uint32_t r;
+  asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+  return r;
+}
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
-  const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
-  return *reinterpret_cast<const uint32_t*>(&h);
+  uint32_t r;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+  return r;
 }
-// Eight consecutive columns (c0 % 8 == 0) of one row: one 16-byte shared store / load.
-__device__ __forceinline__ void st8(__nv_bfloat16* tile, int row, int c0, int rows, const float* v) {
-  const uint4 q = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
-                             pack_bf16x2(v[6], v[7]));
-  *reinterpret_cast<uint4*>(reinterpret_cast<char*>(tile) + kmaj(row, c0, rows)) = q;
+// Sixteen consecutive bf16 columns (c0 % 8 == 0) of one row: two 16-byte shared stores.
+__device__ __forceinline__ void st16(unsigned char* tile, int row, int c0, int rows, const uint32_t* w) {
+  *reinterpret_cast<uint4*>(tile + kmaj(row, c0, rows)) = make_uint4(w[0], w[1], w[2], w[3]);
+  *reinterpret_cast<uint4*>(tile + kmaj(row, c0 + 8, rows)) = make_uint4(w[4], w[5], w[6], w[7]);
 }
-__device__ __forceinline__ void ld8(const __nv_bfloat16* tile, int row, int c0, int rows, float* v) {
-  const uint4 q = *reinterpret_cast<const uint4*>(reinterpret_cast<const char*>(tile) + kmaj(row, c0, rows));
+// Eight consecutive bf16 columns as fp32.
+__device__ __forceinline__ void ld8(const unsigned char* tile, int row, int c0, int rows, float* v) {
+  const uint4 q = *reinterpret_cast<const uint4*>(tile + kmaj(row, c0, rows));
   const uint32_t w[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
@@ -174,32 +234,54 @@ __device__ __forceinline__ float warp_sum(float t) {
   return t;
 }
 
-// Encoding of ray r (or its pre-encoded row).
-__device__ __forceinline__ void encode(const MlpParams& P, int64_t r, float (&f)[kIn]) {
-  if (P.feat) {
-#pragma unroll
-    for (int c = 0; c < kIn; ++c) f[c] = P.feat[r * kIn + c];
-    return;
-  }
-  const float ox = P.rayo[3 * r] - P.cx, oy = P.rayo[3 * r + 1] - P.cy, oz = P.rayo[3 * r + 2] - P.cz;
-  float dx = P.rayd[3 * r], dy = P.rayd[3 * r + 1], dz = P.rayd[3 * r + 2];
-  const float n = sqrtf(dx * dx + dy * dy + dz * dz);
-  const float inv = n > 0.f ? 1.f / n : 0.f;
+// sin(pi x) and cos(pi x): x = n + r with n the nearest integer and |r| <= 1/2 (exact in
+// float), then the Taylor series of sin(pi r) to r^11 and of cos(pi r) to r^12 in Horner
+// form (truncation below 6e-8 on |r| <= 1/2), and the sign (-1)^n.
+__device__ __forceinline__ void sincospi_series(float x, float& s, float& c) {
+  const float n = rintf(x);
+  const float r = x - n;
+  const float r2 = r * r;
+  float ps = fmaf(r2, -0.007370430945714348f, 0.08214588661112819f);
+  ps = fmaf(r2, ps, -0.5992645293207919f);
+  ps = fmaf(r2, ps, 2.550164039877345f);
+  ps = fmaf(r2, ps, -5.167712780049969f);
+  ps = fmaf(r2, ps, 3.141592653589793f);
+  float pc = fmaf(r2, 0.001929574309403922f, -0.02580689139001405f);
+  pc = fmaf(r2, pc, 0.23533063035889312f);
+  pc = fmaf(r2, pc, -1.3352627688545893f);
+  pc = fmaf(r2, pc, 4.058712126416768f);
+  pc = fmaf(r2, pc, -4.934802200544679f);
+  pc = fmaf(r2, pc, 1.f);
+  // |x| < 2^24 here (larger inputs are already integers: r = 0); the parity of n flips both
+  const uint32_t flip = (uint32_t(int(fminf(fabsf(n), 16777216.f))) & 1u) << 31;
+  s = __uint_as_float(__float_as_uint(r * ps) ^ flip);
+  c = __uint_as_float(__float_as_uint(pc) ^ flip);
+}
+
+// The 39 features of one ray, packed as bf16 pairs with zero padding to 48 columns.
+__device__ __forceinline__ void encode_ray(const MlpParams& P, float ox, float oy, float oz, float dx, float dy,
+                                           float dz, uint32_t (&w)[kK0 / 2]) {
+  ox -= P.cx;
+  oy -= P.cy;
+  oz -= P.cz;
+  const float n = __fsqrt_rn(fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
+  const float inv = n > 0.f ? __frcp_rn(n) : 0.f;
   dx *= inv;
   dy *= inv;
   dz *= inv;
-  const float od = ox * dx + oy * dy + oz * dz;
-  float x[3] = {(ox - od * dx) * P.inv_scale, (oy - od * dy) * P.inv_scale, (oz - od * dz) * P.inv_scale};
+  const float od = fmaf(oz, dz, fmaf(oy, dy, ox * dx));
+  float x[3] = {fmaf(-od, dx, ox) * P.inv_scale, fmaf(-od, dy, oy) * P.inv_scale, fmaf(-od, dz, oz) * P.inv_scale};
 #pragma unroll
   for (int i = 0; i < 3; ++i) x[i] = isfinite(x[i]) ? x[i] : 0.f;
-  // sin / cos of 2^q pi x from one sincospi per component and the double-angle identities
-  // sin 2a = 2 sin a cos a, cos 2a = 1 - 2 sin^2 a (after five doublings the error is a
-  // few 1e-6, far below the bf16 rounding the features go through)
+  float f[kK0];
+  // sin / cos of 2^q pi x from the series at the lowest frequency and the double-angle
+  // identities sin 2a = 2 sin a cos a, cos 2a = 1 - 2 sin^2 a (after five doublings the
+  // error is a few 1e-6, far below the bf16 rounding the features go through)
   float sv[3], cv[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
     f[i] = x[i];
-    sincospif(x[i], &sv[i], &cv[i]);
+    sincospi_series(x[i], sv[i], cv[i]);
   }
 #pragma unroll
   for (int q = 0; q < 6; ++q) {
@@ -213,277 +295,431 @@ __device__ __forceinline__ void encode(const MlpParams& P, int64_t r, float (&f)
     }
   }
 #pragma unroll
-  for (int k = 39; k < kIn; ++k) f[k] = 0.f;
+  for (int k = kFeat; k < kK0; ++k) f[k] = 0.f;
+#pragma unroll
+  for (int j = 0; j < kK0 / 2; ++j) w[j] = pack_bf16x2(f[2 * j], f[2 * j + 1]);
+}
+
+// One worker's operand tiles. Inference: a0, then hidden 1 and 2 in h1. Training adds
+// h2 and g3; the backward writes G2 over h2 and G1 over h1.
+template <bool TRAIN>
+struct WorkerTiles {
+  __align__(128) unsigned char a0[kTile * kK0 * 2];  // encoding          [ray][48]
+  __align__(128) unsigned char h1[kTile * kHid * 2];  // hidden 1 / G1     [ray][64]
+};
+template <>
+struct WorkerTiles<true> {
+  __align__(128) unsigned char a0[kTile * kK0 * 2];
+  __align__(128) unsigned char h1[kTile * kHid * 2];
+  __align__(128) unsigned char h2[kTile * kHid * 2];  // hidden 2 / G2     [ray][64]
+  __align__(128) unsigned char g3[kTile * kOut * 2];  // dL/d output       [ray][16]
+};
+
+template <bool TRAIN>
+struct Smem {
+  float b1[kHid], b2[kHid], b3[kOut];
+  float gb3[kMmaWarp][2], loss[kMmaWarp];  // per worker-warp sums (fixed order)
+  uint64_t ready[kWorkers], done[kWorkers];
+  int quit[kWorkers];
+  int abort;   // the MMA warp gave up
+  int failed;  // a wait of this CTA ran out
+  uint32_t tmem_base;
+  __align__(128) unsigned char w1[kHid * kK0 * 2];   // [h1][48]  K-major, rows = output units
+  __align__(128) unsigned char w2[kHid * kHid * 2];  // [h2][h1]
+  __align__(128) unsigned char w3[kOut * kHid * 2];  // [out][h2]
+  __align__(128) unsigned char ones[kOnes * kTile * 2];  // training: all-ones [16][128 rays]
+  WorkerTiles<TRAIN> t[kWorkers];
+};
+
+struct RayIn {
+  float o[3], d[3];
+};
+__device__ __forceinline__ RayIn load_ray(const MlpParams& P, int64_t s) {
+  RayIn x{};
+  if (s < P.num_samples && !P.feat) {
+    const int64_t r = P.sample_idx ? int64_t(__ldg(P.sample_idx + s)) : s;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      x.o[i] = __ldg(P.rayo + 3 * r + i);
+      x.d[i] = __ldg(P.rayd + 3 * r + i);
+    }
+  }
+  return x;
 }
 
 // Inference (TRAIN = false: predictions and cost bins) or the gradients of one training
 // batch (TRAIN = true: each CTA writes its partial gradient and loss to P.partial).
 template <bool TRAIN>
-__global__ void __launch_bounds__(128, TRAIN ? 1 : kInferCtasPerSm) k_mlp(const MlpParams P) {
+__global__ void __launch_bounds__(kThreads, 1) k_mlp(const MlpParams P) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  Smem& S = *reinterpret_cast<Smem*>(smem_raw);
+  Smem<TRAIN>& S = *reinterpret_cast<Smem<TRAIN>*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   constexpr uint32_t kCols = TRAIN ? kColsTrain : kColsInfer;
+  constexpr int kSteps = TRAIN ? kTrainSteps : kInferSteps;
+  const int64_t ntiles = (P.num_samples + kTile - 1) / kTile;
+  const long long wait_limit = P.wait_clocks > 0 ? P.wait_clocks : kWaitClocks;
 
-  // weights into the canonical layouts (8 columns per 16-byte store), biases
+  // weights into the canonical layouts (8 columns per 16-byte store), biases, barriers
   {
     const __nv_bfloat16* w1 = static_cast<const __nv_bfloat16*>(P.w1);
     const __nv_bfloat16* w2 = static_cast<const __nv_bfloat16*>(P.w2);
     const __nv_bfloat16* w3 = static_cast<const __nv_bfloat16*>(P.w3);
-    for (int i = tid; i < kHid * kIn / 8; i += 128) {
-      const int o = i / (kIn / 8), c0 = (i % (kIn / 8)) * 8;
-      *reinterpret_cast<uint4*>(reinterpret_cast<char*>(S.w1) + kmaj(o, c0, kHid)) =
-          *reinterpret_cast<const uint4*>(w1 + o * kIn + c0);
-      *reinterpret_cast<uint4*>(reinterpret_cast<char*>(S.w2) + kmaj(o, c0, kHid)) =
-          *reinterpret_cast<const uint4*>(w2 + o * kHid + c0);
+    for (int i = tid; i < kHid * kK0 / 8; i += kThreads) {
+      const int o = i / (kK0 / 8), c0 = (i % (kK0 / 8)) * 8;
+      *reinterpret_cast<uint4*>(S.w1 + kmaj(o, c0, kHid)) = *reinterpret_cast<const uint4*>(w1 + o * kIn + c0);
     }
-    for (int i = tid; i < kOut * kHid / 8; i += 128) {
+    for (int i = tid; i < kHid * kHid / 8; i += kThreads) {
       const int o = i / (kHid / 8), c0 = (i % (kHid / 8)) * 8;
-      *reinterpret_cast<uint4*>(reinterpret_cast<char*>(S.w3) + kmaj(o, c0, kOut)) =
-          *reinterpret_cast<const uint4*>(w3 + o * kHid + c0);
+      *reinterpret_cast<uint4*>(S.w2 + kmaj(o, c0, kHid)) = *reinterpret_cast<const uint4*>(w2 + o * kHid + c0);
+    }
+    for (int i = tid; i < kOut * kHid / 8; i += kThreads) {
+      const int o = i / (kHid / 8), c0 = (i % (kHid / 8)) * 8;
+      *reinterpret_cast<uint4*>(S.w3 + kmaj(o, c0, kOut)) = *reinterpret_cast<const uint4*>(w3 + o * kHid + c0);
+    }
+    if (TRAIN) {
+      const uint32_t one2 = 0x3F803F80u;  // two bf16 1.0
+      for (int i = tid; i < kOnes * kTile * 2 / 16; i += kThreads)
+        reinterpret_cast<uint4*>(S.ones)[i] = make_uint4(one2, one2, one2, one2);
     }
   }
   if (tid < kHid) {
     S.b1[tid] = P.params[kOffB1 + tid];
     S.b2[tid] = P.params[kOffB2 + tid];
-    for (int w = 0; w < 4; ++w) S.gb1[w][tid] = S.gb2[w][tid] = 0.f;
   }
-  if (tid < kOut) {
-    S.b3[tid] = P.params[kOffB3 + tid];
-    for (int w = 0; w < 4; ++w) S.gb3[w][tid] = 0.f;
+  if (tid < kOut) S.b3[tid] = P.params[kOffB3 + tid];
+  if (tid < kMmaWarp) {
+    S.gb3[tid][0] = S.gb3[tid][1] = 0.f;
+    S.loss[tid] = 0.f;
   }
-  if (tid < 4) S.loss[tid] = 0.f;
-  if (warp == 0) {
+  if (tid < kWorkers) S.quit[tid] = 0;
+  if (tid == 0) {
+    S.abort = 0;
+    S.failed = 0;
+    for (int w = 0; w < kWorkers; ++w) {
+      mbar_init(&S.ready[w], 1);
+      mbar_init(&S.done[w], 1);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == kMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem_base)),
                  "r"(kCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&S.bar)), "r"(1));
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
+  fence_async_smem();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = S.tmem_base;
-  const uint32_t lane_off = uint32_t(warp * 32) << 16;  // TMEM lanes of this warp's quarter
-  uint32_t phase = 0, pending = 0;
   bool ok = true;
-  int tiles_done = 0;
 
-  // Make the generic shared stores visible to the tensor cores, let thread 0 issue the
-  // MMAs and commit them, wait (bounded) for completion. False on timeout.
-  auto run = [&](auto issue) -> bool {
-    fence_async_smem();
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    if (tid == 0) {
-      issue();
-      mma_commit(&S.bar);
+  if (warp == kMmaWarp) {
+    // ---- MMA warp: one thread serves the workers' requests in round-robin order
+    if (lane == 0) {
+      int64_t left[kWorkers];
+      uint32_t rphase[kWorkers];
+      int step[kWorkers];
+      int64_t total = 0;
+      for (int w = 0; w < kWorkers; ++w) {
+        const int64_t first = int64_t(blockIdx.x) * kWorkers + w, stride = int64_t(gridDim.x) * kWorkers;
+        left[w] = first < ntiles ? ((ntiles - 1 - first) / stride + 1) * kSteps : 0;
+        total += left[w];
+        rphase[w] = 0;
+        step[w] = 0;
+      }
+      bool gw3_started = false, gw2_started = false, gw1_started = false;  // first MMA overwrites
+      const uint32_t sw1 = smem_u32(S.w1), sw2 = smem_u32(S.w2), sw3 = smem_u32(S.w3), sones = smem_u32(S.ones);
+      while (total > 0 && ok) {
+        for (int w = 0; w < kWorkers && ok; ++w) {
+          if (left[w] == 0) continue;
+          // wait for the worker's operands (bounded; a worker that gave up stops being served)
+          const long long t0 = clock64();
+          bool got = false;
+          while (!(got = mbar_try(&S.ready[w], rphase[w]))) {
+            if (*reinterpret_cast<volatile int*>(&S.quit[w])) break;
+            if (clock64() - t0 > kWaitClocks) {
+              ok = false;
+              break;
+            }
+          }
+          if (!got) {
+            total -= left[w];
+            left[w] = 0;
+            continue;
+          }
+          rphase[w] ^= 1u;
+          tc_fence_after();
+          const uint32_t d = tmem + 64u * uint32_t(w);
+          const uint32_t sa0 = smem_u32(S.t[w].a0), sh1 = smem_u32(S.t[w].h1);
+          const int q = step[w];
+          if (q == 0) {  // layer 1: D = A0 W1^T
+            for (int ks = 0; ks < kK0 / 16; ++ks)
+              mma(d, desc_k(sa0, kTile, ks), desc_k(sw1, kHid, ks), idesc(128, kHid, false, false), ks > 0);
+          } else if (q == 1) {  // layer 2: D = H1 W2^T
+            for (int ks = 0; ks < kHid / 16; ++ks)
+              mma(d, desc_k(sh1, kTile, ks), desc_k(sw2, kHid, ks), idesc(128, kHid, false, false), ks > 0);
+          } else if (q == 2) {  // layer 3: D[., 0:16] = H2 W3^T (inference keeps H2 in h1)
+            const uint32_t sh2 = TRAIN ? smem_u32(reinterpret_cast<WorkerTiles<true>&>(S.t[w]).h2) : sh1;
+            for (int ks = 0; ks < kHid / 16; ++ks)
+              mma(d, desc_k(sh2, kTile, ks), desc_k(sw3, kOut, ks), idesc(128, kOut, false, false), ks > 0);
+          } else if (TRAIN) {
+            WorkerTiles<true>& T = reinterpret_cast<WorkerTiles<true>&>(S.t[w]);
+            const uint32_t sh2 = smem_u32(T.h2), sg3 = smem_u32(T.g3);
+            if (q == 3) {
+              // dA2[128 x 64] = G3[128 x 16] W3[16 x 64] (W3 read MN-major: MN = h2, K = out)
+              mma(d, desc_k(sg3, kTile, 0), desc_mn(sw3, kOut, 0), idesc(128, kHid, false, true), 0);
+              // dW3^T[h2][out] += A2^T G3 (both tiles MN-major, K = ray)
+              for (int ks = 0; ks < kTile / 16; ++ks)
+                mma(tmem + kColGW3, desc_mn(sh2, kTile, ks), desc_mn(sg3, kTile, ks), idesc(64, kOut, true, true),
+                    uint32_t(ks > 0 || gw3_started));
+              gw3_started = true;
+            } else if (q == 4) {
+              // dA1 = G2 W2 (W2 MN-major: MN = h1, K = h2); G2 lives in h2
+              for (int ks = 0; ks < kHid / 16; ++ks)
+                mma(d, desc_k(sh2, kTile, ks), desc_mn(sw2, kHid, ks), idesc(128, kHid, false, true), ks > 0);
+              for (int ks = 0; ks < kTile / 16; ++ks) {
+                const uint32_t acc = uint32_t(ks > 0 || gw2_started);
+                // dW2[h2][h1] += G2^T A1
+                mma(tmem + kColGW2, desc_mn(sh2, kTile, ks), desc_mn(sh1, kTile, ks), idesc(64, kHid, true, true), acc);
+                // db2 (every column) += G2^T 1
+                mma(tmem + kColGB2, desc_mn(sh2, kTile, ks), desc_k(sones, kOnes, ks), idesc(64, kOnes, true, false),
+                    acc);
+              }
+              gw2_started = true;
+            } else {
+              // G1 lives in h1: dW1[h1][0:48] += G1^T A0, db1 += G1^T 1
+              for (int ks = 0; ks < kTile / 16; ++ks) {
+                const uint32_t acc = uint32_t(ks > 0 || gw1_started);
+                mma(tmem + kColGW1, desc_mn(sh1, kTile, ks), desc_mn(sa0, kTile, ks), idesc(64, kK0, true, true), acc);
+                mma(tmem + kColGB1, desc_mn(sh1, kTile, ks), desc_k(sones, kOnes, ks), idesc(64, kOnes, true, false),
+                    acc);
+              }
+              gw1_started = true;
+            }
+          }
+          mma_commit(&S.done[w]);
+          step[w] = step[w] + 1 == kSteps ? 0 : step[w] + 1;
+          --left[w];
+          --total;
+        }
+      }
+      if (!ok) {
+        atomicExch(P.error, 1);
+        *reinterpret_cast<volatile int*>(&S.abort) = 1;
+        *reinterpret_cast<volatile int*>(&S.failed) = 1;
+      }
     }
-    pending = phase;
-    const bool got = mbar_wait(&S.bar, phase, P.wait_clocks > 0 ? P.wait_clocks : kWaitClocks);
-    phase ^= 1u;
-    tc_fence_after();
-    return __syncthreads_and(got) != 0;
-  };
+    __syncwarp();
+  } else {
+    // ---- worker warpgroup g: rows of its tiles = its 128 threads; TMEM lanes = rows
+    const int g = warp >> 2, row = tid & 127;
+    const uint32_t lanes = uint32_t((warp & 3) * 32) << 16;
+    const uint32_t dcol = tmem + lanes + 64u * uint32_t(g);
+    WorkerTiles<TRAIN>& T = S.t[g];
+    uint32_t dphase = 0;  // phase of the next completion on done[g]
+    const int64_t stride = int64_t(gridDim.x) * kWorkers;
+    int64_t tile = int64_t(blockIdx.x) * kWorkers + g;
+    RayIn next = load_ray(P, tile * kTile + row);
+    bool first = true;
 
-  // inference: hidden 1 and 2 overwrite the tile the previous (completed) MMA read
-  __nv_bfloat16* const a1 = TRAIN ? S.a1 : S.a0;
-  __nv_bfloat16* const a2 = TRAIN ? S.a2 : S.a0;
-  constexpr uint32_t kColH2 = TRAIN ? kColD2 : kColD1;  // inference: layers 2 and 3 reuse D1's columns
-  constexpr uint32_t kColY = TRAIN ? kColD3 : kColD1;
-  const uint32_t sa0 = smem_u32(S.a0), sa1 = smem_u32(a1), sa2 = smem_u32(a2);
-  const uint32_t sw1 = smem_u32(S.w1), sw2 = smem_u32(S.w2), sw3 = smem_u32(S.w3);
-  const uint32_t sg1 = smem_u32(S.g1), sg2 = smem_u32(S.g2), sg3 = smem_u32(S.g3);
-  const int64_t ntiles = (P.num_samples + kTile - 1) / kTile;
+    // bounded wait for the next completion of this worker's MMAs; every thread of the
+    // warpgroup gets the same answer
+    auto await_mma = [&]() -> bool {
+      const bool got = mbar_wait(&S.done[g], dphase, wait_limit);
+      dphase ^= 1u;
+      tc_fence_after();
+      return worker_and(g, got);
+    };
+    // hand the operand tiles to the MMA warp
+    auto hand_over = [&]() {
+      fence_async_smem();
+      tc_fence_before();
+      worker_sync(g);
+      if (row == 0) mbar_arrive(&S.ready[g]);
+    };
 
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int64_t s = tile * kTile + tid;
-    const bool valid = s < P.num_samples;
-    const int64_t r = valid ? (P.sample_idx ? int64_t(P.sample_idx[s]) : s) : 0;
-    {
-      float f[kIn];
-      encode(P, r, f);
-      if (!valid)
+    for (; tile < ntiles && ok; tile += stride) {
+      const int64_t s = tile * kTile + row;
+      const bool valid = s < P.num_samples;
+      const int64_t r = valid ? (P.sample_idx ? int64_t(__ldg(P.sample_idx + s)) : s) : 0;
+      // ---- encoding
+      uint32_t enc[kK0 / 2];
+      if (P.feat) {
+        float f[kK0];
 #pragma unroll
-        for (int c = 0; c < kIn; ++c) f[c] = 0.f;
+        for (int c = 0; c < kK0; ++c) f[c] = (valid && c < kFeat) ? __ldg(P.feat + r * kIn + c) : 0.f;
 #pragma unroll
-      for (int c0 = 0; c0 < kIn; c0 += 8) st8(S.a0, tid, c0, kTile, f + c0);
-    }
-    // layer 1: D1[128 x 64] = A0 W1^T
-    ok = run([&] {
-      for (int ks = 0; ks < kIn / 16; ++ks)
-        mma(tmem + kColD1, desc_k(sa0, kTile, ks), desc_k(sw1, kHid, ks), idesc(128, kHid, false, false), ks > 0);
-    });
-    if (!ok) break;
+        for (int j = 0; j < kK0 / 2; ++j) enc[j] = pack_bf16x2(f[2 * j], f[2 * j + 1]);
+      } else {
+        encode_ray(P, next.o[0], next.o[1], next.o[2], next.d[0], next.d[1], next.d[2], enc);
+        if (!valid)
 #pragma unroll
-    for (int c0 = 0; c0 < kHid; c0 += 16) {
-      float v[16];
-      tmem_ld16(tmem + lane_off + kColD1 + c0, v);
+          for (int j = 0; j < kK0 / 2; ++j) enc[j] = 0u;
+        next = load_ray(P, (tile + stride) * kTile + row);  // in flight during this tile's MMAs
+      }
+      // training: the previous tile's weight-gradient MMAs read a0 and h1
+      if (TRAIN && !first && !(ok = await_mma())) break;
+      first = false;
 #pragma unroll
-      for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i] + S.b1[c0 + i], 0.f);
-      st8(a1, tid, c0, kTile, v);
-      st8(a1, tid, c0 + 8, kTile, v + 8);
-    }
-    // layer 2: D2 = A1 W2^T
-    ok = run([&] {
-      for (int ks = 0; ks < kHid / 16; ++ks)
-        mma(tmem + kColH2, desc_k(sa1, kTile, ks), desc_k(sw2, kHid, ks), idesc(128, kHid, false, false), ks > 0);
-    });
-    if (!ok) break;
+      for (int c = 0; c < kK0 / 8; ++c)
+        *reinterpret_cast<uint4*>(T.a0 + kmaj(row, 8 * c, kTile)) =
+            make_uint4(enc[4 * c], enc[4 * c + 1], enc[4 * c + 2], enc[4 * c + 3]);
+      // ---- layers 1 and 2: bias, ReLU, bf16 into the next operand tile
+#pragma unroll 1
+      for (int layer = 0; layer < 2 && ok; ++layer) {
+        hand_over();
+        if (!(ok = await_mma())) break;
+        const float* b = layer == 0 ? S.b1 : S.b2;
+        unsigned char* dst = (TRAIN && layer == 1) ? reinterpret_cast<WorkerTiles<true>&>(T).h2 : T.h1;
 #pragma unroll
-    for (int c0 = 0; c0 < kHid; c0 += 16) {
-      float v[16];
-      tmem_ld16(tmem + lane_off + kColH2 + c0, v);
+        for (int half = 0; half < 2; ++half) {  // 32 columns at a time (registers)
+          float v[32];
+          tmem_ld<32>(dcol + 32 * half, v);
+          uint32_t h[16];
 #pragma unroll
-      for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i] + S.b2[c0 + i], 0.f);
-      st8(a2, tid, c0, kTile, v);
-      st8(a2, tid, c0 + 8, kTile, v + 8);
-    }
-    // layer 3: D3[128 x 16] = A2 W3^T
-    ok = run([&] {
-      for (int ks = 0; ks < kHid / 16; ++ks)
-        mma(tmem + kColY, desc_k(sa2, kTile, ks), desc_k(sw3, kOut, ks), idesc(128, kOut, false, false), ks > 0);
-    });
-    if (!ok) break;
-    float y[16];
-    tmem_ld16(tmem + lane_off + kColY, y);
-    const float y0 = y[0] + S.b3[0], y1 = y[1] + S.b3[1];
-    ++tiles_done;
-    if (!TRAIN) {
+          for (int j = 0; j < 8; ++j) {
+            const float4 bb = *reinterpret_cast<const float4*>(b + 32 * half + 4 * j);
+            h[2 * j] = bias_relu_bf16x2(v[4 * j], v[4 * j + 1], bb.x, bb.y);
+            h[2 * j + 1] = bias_relu_bf16x2(v[4 * j + 2], v[4 * j + 3], bb.z, bb.w);
+          }
+#pragma unroll
+          for (int c = 0; c < 2; ++c) st16(dst, row, 32 * half + 16 * c, kTile, h + 8 * c);
+        }
+      }
+      if (!ok) break;
+      // ---- layer 3
+      hand_over();
+      if (!(ok = await_mma())) break;
+      float y2[2];
+      tmem_ld<2>(dcol, y2);
+      const float y0 = y2[0] + S.b3[0], y1 = y2[1] + S.b3[1];
+      if (!TRAIN) {
+        if (valid) {
+          *reinterpret_cast<float2*>(P.pred + 2 * r) = make_float2(y0, y1);
+          if (P.bins) P.bins[r] = uint8_t(int(y0 > P.thr[0]) + int(y0 > P.thr[1]) + int(y0 > P.thr[2]));
+        }
+        continue;
+      }
+      // ---- training: weighted squared error on the two outputs, mean over the batch
+      WorkerTiles<true>& TT = reinterpret_cast<WorkerTiles<true>&>(T);
+      float g0 = 0.f, g1 = 0.f, l = 0.f;
       if (valid) {
-        P.pred[2 * r] = y0;
-        P.pred[2 * r + 1] = y1;
-        if (P.bins) P.bins[r] = uint8_t(int(y0 > P.thr[0]) + int(y0 > P.thr[1]) + int(y0 > P.thr[2]));
+        const float e0 = y0 - P.target[2 * r], e1 = y1 - P.target[2 * r + 1];
+        g0 = 2.f * P.loss_w0 * e0 * P.inv_batch;
+        g1 = 2.f * P.loss_w1 * e1 * P.inv_batch;
+        l = (P.loss_w0 * e0 * e0 + P.loss_w1 * e1 * e1) * P.inv_batch;
       }
-      continue;
-    }
-    // ---- training: weighted squared error on the two outputs, mean over the batch
-    float g[16] = {};
-    float l = 0.f;
-    if (valid) {
-      const float e0 = y0 - P.target[2 * r], e1 = y1 - P.target[2 * r + 1];
-      g[0] = 2.f * P.loss_w0 * e0 * P.inv_batch;
-      g[1] = 2.f * P.loss_w1 * e1 * P.inv_batch;
-      l = (P.loss_w0 * e0 * e0 + P.loss_w1 * e1 * e1) * P.inv_batch;
-    }
-    st8(S.g3, tid, 0, kTile, g);
-    st8(S.g3, tid, 8, kTile, g + 8);
-    {
-      const float t0 = warp_sum(g[0]), t1 = warp_sum(g[1]), tl = warp_sum(l);
-      if (lane == 0) {
-        S.gb3[warp][0] += t0;
-        S.gb3[warp][1] += t1;
-        S.loss[warp] += tl;
+      {
+        const uint32_t gz[8] = {pack_bf16x2(g0, g1), 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+        st16(TT.g3, row, 0, kTile, gz);
+        const float t0 = warp_sum(g0), t1 = warp_sum(g1), tl = warp_sum(l);
+        if (lane == 0) {
+          S.gb3[warp][0] += t0;
+          S.gb3[warp][1] += t1;
+          S.loss[warp] += tl;
+        }
       }
-    }
-    // dA2[128 x 64] = G3[128 x 16] W3[16 x 64]; W3 read MN-major (MN = h2, K = out)
-    ok = run([&] {
-      mma(tmem + kColD2, desc_k(sg3, kTile, 0), desc_mn(sw3, kOut, 0), idesc(128, kHid, false, true), 0);
-    });
-    if (!ok) break;
+      // ---- dA2 = G3 W3 (and dW3): G2 = dA2 masked by A2 > 0, written over A2;
+      // then dA1 = G2 W2 (and dW2, db2): G1 = dA1 masked by A1 > 0, written over A1
+#pragma unroll 1
+      for (int back = 0; back < 2 && ok; ++back) {
+        hand_over();
+        if (!(ok = await_mma())) break;
+        unsigned char* act = back == 0 ? TT.h2 : TT.h1;
 #pragma unroll
-    for (int c0 = 0; c0 < kHid; c0 += 16) {
-      float v[16], a[16];
-      tmem_ld16(tmem + lane_off + kColD2 + c0, v);
-      ld8(S.a2, tid, c0, kTile, a);
-      ld8(S.a2, tid, c0 + 8, kTile, a + 8);
+        for (int half = 0; half < 2; ++half) {
+          float v[32];
+          tmem_ld<32>(dcol + 32 * half, v);
+          uint32_t h[16];
 #pragma unroll
-      for (int i = 0; i < 16; ++i) v[i] = a[i] > 0.f ? v[i] : 0.f;
-      st8(S.g2, tid, c0, kTile, v);
-      st8(S.g2, tid, c0 + 8, kTile, v + 8);
+          for (int c = 0; c < 4; ++c) {
+            float a[8];
+            ld8(act, row, 32 * half + 8 * c, kTile, a);
 #pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const float t = warp_sum(v[i]);
-        if (lane == 0) S.gb2[warp][c0 + i] += t;
+            for (int i = 0; i < 4; ++i)
+              h[4 * c + i] = pack_bf16x2(a[2 * i] > 0.f ? v[8 * c + 2 * i] : 0.f,
+                                         a[2 * i + 1] > 0.f ? v[8 * c + 2 * i + 1] : 0.f);
+          }
+#pragma unroll
+          for (int c = 0; c < 2; ++c) st16(act, row, 32 * half + 16 * c, kTile, h + 8 * c);
+        }
       }
+      if (!ok) break;
+      // ---- dW1, db1: handed over now, waited for before a0 / h1 are overwritten
+      hand_over();
     }
-    // dA1[128 x 64] = G2[128 x 64] W2[64 x 64]; W2 read MN-major (MN = h1, K = h2)
-    ok = run([&] {
-      for (int ks = 0; ks < kHid / 16; ++ks)
-        mma(tmem + kColD1, desc_k(sg2, kTile, ks), desc_mn(sw2, kHid, ks), idesc(128, kHid, false, true), ks > 0);
-    });
-    if (!ok) break;
-#pragma unroll
-    for (int c0 = 0; c0 < kHid; c0 += 16) {
-      float v[16], a[16];
-      tmem_ld16(tmem + lane_off + kColD1 + c0, v);
-      ld8(S.a1, tid, c0, kTile, a);
-      ld8(S.a1, tid, c0 + 8, kTile, a + 8);
-#pragma unroll
-      for (int i = 0; i < 16; ++i) v[i] = a[i] > 0.f ? v[i] : 0.f;
-      st8(S.g1, tid, c0, kTile, v);
-      st8(S.g1, tid, c0 + 8, kTile, v + 8);
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const float t = warp_sum(v[i]);
-        if (lane == 0) S.gb1[warp][c0 + i] += t;
-      }
+    // training: the last tile's weight-gradient MMAs
+    if (TRAIN && ok && !first) ok = await_mma();
+    if (!ok) {
+      atomicExch(P.error, 1);
+      *reinterpret_cast<volatile int*>(&S.failed) = 1;
+      // let this worker's MMAs in flight finish (bounded, at the full limit) before TMEM is
+      // freed, unless the MMA warp itself gave up
+      if (!*reinterpret_cast<volatile int*>(&S.abort)) mbar_wait(&S.done[g], dphase ^ 1u, kWaitClocks);
+      worker_sync(g);
+      if (row == 0) *reinterpret_cast<volatile int*>(&S.quit[g]) = 1;
     }
-    // Weight gradients, reduced over the tile's 128 rays (K) and accumulated over this
-    // CTA's tiles in TMEM (M = 64). Both operands are tiles read MN-major (K = ray).
-    const uint32_t acc = tiles_done > 1 ? 1u : 0u;
-    ok = run([&] {
-      for (int ks = 0; ks < kTile / 16; ++ks) {
-        const uint32_t a = uint32_t(ks > 0) | acc;
-        // dW1[h1][in] += G1^T A0
-        mma(tmem + kColGW1, desc_mn(sg1, kTile, ks), desc_mn(sa0, kTile, ks), idesc(64, kIn, true, true), a);
-        // dW2[h2][h1] += G2^T A1
-        mma(tmem + kColGW2, desc_mn(sg2, kTile, ks), desc_mn(sa1, kTile, ks), idesc(64, kHid, true, true), a);
-        // dW3^T[h2][out] += A2^T G3
-        mma(tmem + kColGW3, desc_mn(sa2, kTile, ks), desc_mn(sg3, kTile, ks), idesc(64, kOut, true, true), a);
-      }
-    });
-    if (!ok) break;
   }
 
-  if (TRAIN && ok && tiles_done > 0) {
-    // M = 64 accumulators: row m lives in TMEM lane (m % 16) + 32 (m / 16), so lanes 0..15
-    // of warp w hold rows 16 w .. 16 w + 15.
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const bool cta_ok = *reinterpret_cast<volatile int*>(&S.failed) == 0;
+  if (TRAIN && cta_ok && warp < 4) {
+    // worker 0's warps read the M = 64 accumulators: row m lives in TMEM lane (m % 16) +
+    // 32 (m / 16), so lanes 0..15 of warp w hold rows 16 w .. 16 w + 15
     float* out = P.partial + int64_t(blockIdx.x) * (kMlpParams + 1);
+    const uint32_t lanes = uint32_t(warp * 32) << 16;
     const int m = warp * 16 + lane;
+    const bool any = int64_t(blockIdx.x) * kWorkers < ntiles;  // this CTA had tiles
 #pragma unroll
     for (int c0 = 0; c0 < kIn; c0 += 16) {
       float v[16];
-      tmem_ld16(tmem + lane_off + kColGW1 + c0, v);
+      if (c0 < kK0) tmem_ld<16>(tmem + lanes + kColGW1 + c0, v);
       if (lane < 16)
 #pragma unroll
-        for (int i = 0; i < 16; ++i) out[kOffW1 + m * kIn + c0 + i] = v[i];
+        for (int i = 0; i < 16; ++i) out[kOffW1 + m * kIn + c0 + i] = (any && c0 < kK0) ? v[i] : 0.f;
     }
 #pragma unroll
     for (int c0 = 0; c0 < kHid; c0 += 16) {
       float v[16];
-      tmem_ld16(tmem + lane_off + kColGW2 + c0, v);
+      tmem_ld<16>(tmem + lanes + kColGW2 + c0, v);
       if (lane < 16)
 #pragma unroll
-        for (int i = 0; i < 16; ++i) out[kOffW2 + m * kHid + c0 + i] = v[i];
+        for (int i = 0; i < 16; ++i) out[kOffW2 + m * kHid + c0 + i] = any ? v[i] : 0.f;
     }
     {
       float v[16];
-      tmem_ld16(tmem + lane_off + kColGW3, v);  // dW3^T: row m = h2, column = output
+      tmem_ld<16>(tmem + lanes + kColGW3, v);  // dW3^T: row m = h2, column = output
       if (lane < 16)
 #pragma unroll
-        for (int i = 0; i < kOut; ++i) out[kOffW3 + i * kHid + m] = v[i];
+        for (int i = 0; i < kOut; ++i) out[kOffW3 + i * kHid + m] = any ? v[i] : 0.f;
     }
-    __syncthreads();
-    if (tid < kHid) {
-      out[kOffB1 + tid] = ((S.gb1[0][tid] + S.gb1[1][tid]) + S.gb1[2][tid]) + S.gb1[3][tid];
-      out[kOffB2 + tid] = ((S.gb2[0][tid] + S.gb2[1][tid]) + S.gb2[2][tid]) + S.gb2[3][tid];
+    {
+      float v1[16], v2[16];
+      tmem_ld<16>(tmem + lanes + kColGB1, v1);
+      tmem_ld<16>(tmem + lanes + kColGB2, v2);
+      if (lane < 16) {
+        out[kOffB1 + m] = any ? v1[0] : 0.f;
+        out[kOffB2 + m] = any ? v2[0] : 0.f;
+      }
     }
-    if (tid < kOut) out[kOffB3 + tid] = ((S.gb3[0][tid] + S.gb3[1][tid]) + S.gb3[2][tid]) + S.gb3[3][tid];
-    if (tid == 0) out[kMlpParams] = ((S.loss[0] + S.loss[1]) + S.loss[2]) + S.loss[3];
-  }
-  if (!ok) {
-    // let MMAs still in flight finish (bounded, at the full limit) before TMEM is freed
-    mbar_wait(&S.bar, pending, kWaitClocks);
-    if (tid == 0) atomicExch(P.error, 1);
+    if (tid < kOut) {
+      float t = 0.f;
+      if (tid < 2)
+        for (int w = 0; w < kMmaWarp; ++w) t += S.gb3[w][tid];
+      out[kOffB3 + tid] = t;
+    }
+    if (tid == 0) {
+      float t = 0.f;
+      for (int w = 0; w < kMmaWarp; ++w) t += S.loss[w];
+      out[kMlpParams] = t;
+    }
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
+  if (warp == kMmaWarp) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
 }
 
 // Sum of the per-CTA partial gradients (and losses) in CTA order.
@@ -528,31 +764,38 @@ __global__ void k_mlp_pack(const float* __restrict__ params, __nv_bfloat16* __re
 static_assert(kOffW2 == kOffW1 + kHid * kIn && kOffW3 == kOffW2 + kHid * kHid && kOffB1 == kOffW3 + kOut * kHid &&
                   kOffB2 == kOffB1 + kHid && kOffB3 == kOffB2 + kHid && kMlpParams == kOffB3 + kOut,
               "parameter block layout");
-static_assert(sizeof(Smem) + 128 <= kTrainSmem, "training shared memory");
-constexpr size_t kInferSmem = offsetof(Smem, a1) + 128;
-static_assert(kInferCtasPerSm * (kInferSmem + 1024) <= 228 * 1024, "inference CTAs per SM");
-static_assert(kInferCtasPerSm * kColsInfer <= 512, "inference TMEM columns per SM");
-static_assert(offsetof(Smem, w1) % 128 == 0 && offsetof(Smem, a0) % 128 == 0 && offsetof(Smem, a1) % 128 == 0,
+constexpr size_t kInferSmem = sizeof(Smem<false>) + 128;
+constexpr size_t kTrainSmem = sizeof(Smem<true>) + 128;
+static_assert(kTrainSmem <= 227 * 1024, "training shared memory");
+static_assert(kInferSmem <= 227 * 1024, "inference shared memory");
+static_assert(kWorkers * 64 <= int(kColsInfer) && kColGB2 + kOnes <= kColsTrain && kWorkers * 64 <= int(kColGW1),
+              "tensor-memory columns");
+static_assert(offsetof(Smem<true>, w1) % 128 == 0 && offsetof(Smem<true>, t) % 128 == 0 &&
+                  offsetof(Smem<false>, t) % 128 == 0 && sizeof(WorkerTiles<true>) % 128 == 0 &&
+                  sizeof(WorkerTiles<false>) % 128 == 0,
               "tiles aligned");
-static_assert(kmaj(127, 63, 128) + 2 == kTile * kIn * 2, "tile layout covers the tile");
+static_assert(kmaj(127, 63, 128) + 2 == kTile * kHid * 2 && kmaj(127, 47, 128) + 2 == kTile * kK0 * 2,
+              "tile layout covers the tile");
+static_assert(kThreads <= 1024 && kWorkers <= 15, "block size and named barriers");
 
 }  // namespace
 
-cudaError_t launch_mlp(const MlpParams& P, bool train, int max_grid, cudaStream_t st) {
+int mlp_grid(int64_t num_samples, int max_grid, bool train) {
+  const int64_t ntiles = (num_samples + kTile - 1) / kTile;
+  // training: two tiles per worker, so the warpgroups of a CTA overlap their steps; inference:
+  // every SM, as many tiles per worker as it takes
+  const int64_t per_cta = train ? 2 * kWorkers : kWorkers;
+  return int(std::max<int64_t>(1, std::min<int64_t>((ntiles + per_cta - 1) / per_cta, max_grid)));
+}
+
+cudaError_t launch_mlp(const MlpParams& P, bool train, int grid, cudaStream_t st) {
   if (P.num_samples == 0) return cudaSuccess;
   const size_t smem = train ? kTrainSmem : kInferSmem;
   auto kern = train ? k_mlp<true> : k_mlp<false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
-  const int64_t ntiles = (P.num_samples + kTile - 1) / kTile;
-  const int g = int(std::max<int64_t>(1, std::min<int64_t>(ntiles, max_grid)));
-  kern<<<g, 128, smem, st>>>(P);
+  kern<<<grid, kThreads, smem, st>>>(P);
   return cudaGetLastError();
-}
-
-int mlp_grid(int64_t num_samples, int max_grid) {
-  const int64_t ntiles = (num_samples + kTile - 1) / kTile;
-  return int(std::max<int64_t>(1, std::min<int64_t>(ntiles, max_grid)));
 }
 
 cudaError_t launch_mlp_reduce(const float* partial, int grid, float* grads, float* loss, cudaStream_t st) {

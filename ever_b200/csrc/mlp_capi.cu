@@ -65,8 +65,8 @@ int ever_mlp_predict(const EverMlp* mlp, const float* rayo, const float* rayd, c
   if (bins)
     for (int i = 0; i < 3; ++i) P.thr[i] = thresholds[i];
   P.error = error;
-  return cuda_status(ever::launch_mlp(P, false, ever::kMlpInferCtasPerSm * sm_count(), static_cast<cudaStream_t>(stream)),
-                     "ever_mlp_predict");
+  const int grid = ever::mlp_grid(num_rays, sm_count(), false);
+  return cuda_status(ever::launch_mlp(P, false, grid, static_cast<cudaStream_t>(stream)), "ever_mlp_predict");
 }
 
 int ever_mlp_gradients(const EverMlp* mlp, const float* rayo, const float* rayd, const float* feat,
@@ -93,7 +93,7 @@ int ever_mlp_gradients(const EverMlp* mlp, const float* rayo, const float* rayd,
   P.inv_batch = 1.f / float(num_samples);
   P.partial = static_cast<float*>(workspace);
   P.error = error;
-  const int grid = ever::mlp_grid(num_samples, std::min(sm_count(), ever::kMlpMaxGrid));
+  const int grid = ever::mlp_grid(num_samples, std::min(sm_count(), ever::kMlpMaxGrid), true);
   cudaError_t e = ever::launch_mlp(P, true, grid, st);
   if (e == cudaSuccess) e = ever::launch_mlp_reduce(P.partial, grid, grads, loss, st);
   return cuda_status(e, "ever_mlp_gradients");

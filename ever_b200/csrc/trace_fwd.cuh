@@ -537,14 +537,8 @@ __device__ __forceinline__ bool run_rounds(const SceneRef& sc, const TraceCtx& C
 // continue it from there (lower = that event's key), so the results do not depend on it.
 constexpr int kFrontierCap = 384;  // nodes per breadth-first level
 constexpr int kCandCap = 512;      // leaves per packet (a power of two: the sort's width)
-constexpr int kLeafGroup = 4;      // leaves tested together before their events are inserted
-constexpr float kFirstStage = 1.0f;  // the first stage's share of the packet's t extent
-constexpr int kMaxHalvings = 24;     // halvings of an overflowing range before the rounds take over
-constexpr int kMaxWalks = 64;        // breadth-first walks per packet before the rounds take over
-// Shared ints per warp: the traversal stack, two frontier levels, the leaf keys (64-bit),
-// the packet's bounds between stages.
-constexpr int kBoundsInts = 20;
-constexpr int kWarpInts = kStackDepth + 2 * kFrontierCap + 2 * kCandCap + kBoundsInts;
+// Shared ints per warp: the traversal stack, two frontier levels, the leaf keys (64-bit).
+constexpr int kWarpInts = kStackDepth + 2 * kFrontierCap + 2 * kCandCap;
 
 __device__ __forceinline__ uint32_t ordered_bits(float f) {
   const uint32_t u = __float_as_uint(f);
@@ -585,15 +579,15 @@ __device__ __forceinline__ PacketBounds packet_bounds(const Ray& ray, const RayS
 __device__ __forceinline__ float min4(float a, float b, float c, float d) { return fminf(fminf(a, b), fminf(c, d)); }
 __device__ __forceinline__ float max4(float a, float b, float c, float d) { return fmaxf(fmaxf(a, b), fmaxf(c, d)); }
 
-// Bounds of the t range over which any packet ray can be inside the box, within
-// [t_lo, t_hi]; false when no packet ray meets the box there. Interval products bound every ray's plane
+// A lower bound of the t at which any packet ray enters the box within [0, cap], or +inf
+// when no packet ray can meet it there. Interval products bound every ray's plane
 // distances; the float rounding of the bound (a few ulps) is covered by widening it by a
 // relative 1e-6. Axes whose direction changes sign bound no t: there the positions the
 // packet reaches over the t range of the other axes must overlap the box.
-__device__ __forceinline__ bool packet_span(const PacketBounds& P, float lx, float ly, float lz, float hx, float hy,
-                                            float hz, float t_lo, float t_hi, float& tn_out, float& tf_out) {
+__device__ __forceinline__ float packet_entry(const PacketBounds& P, float lx, float ly, float lz, float hx, float hy,
+                                              float hz, float cap) {
   const float lo[3] = {lx, ly, lz}, hi[3] = {hx, hy, hz};
-  float tn = t_lo, tf = t_hi;
+  float tn = 0.f, tf = cap;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     if (P.free_axes >> a & 1u) continue;
@@ -606,7 +600,7 @@ __device__ __forceinline__ bool packet_span(const PacketBounds& P, float lx, flo
   }
   tn = tn - 1e-6f * fabsf(tn);
   tf = tf + 1e-6f * fabsf(tf);
-  if (!(tn <= tf)) return false;
+  if (!(tn <= tf)) return INFINITY;
   if (P.free_axes) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -614,27 +608,17 @@ __device__ __forceinline__ bool packet_span(const PacketBounds& P, float lx, flo
       const float xl = P.omin[a] + min4(tn * P.dmin[a], tn * P.dmax[a], tf * P.dmin[a], tf * P.dmax[a]);
       const float xh = P.omax[a] + max4(tn * P.dmin[a], tn * P.dmax[a], tf * P.dmin[a], tf * P.dmax[a]);
       const float tol = 1e-6f * (fabsf(xl) + fabsf(xh) + fabsf(tf));
-      if (xh + tol < lo[a] || xl - tol > hi[a]) return false;
+      if (xh + tol < lo[a] || xl - tol > hi[a]) return INFINITY;
     }
   }
-  tn_out = fmaxf(tn, 0.f);
-  tf_out = tf;
-  return true;
-}
-
-// A lower bound of the t at which any packet ray enters the box within [t_lo, t_hi], or
-// +inf when no packet ray can meet it there.
-__device__ __forceinline__ float packet_entry(const PacketBounds& P, float lx, float ly, float lz, float hx, float hy,
-                                              float hz, float t_lo, float t_hi) {
-  float tn, tf;
-  return packet_span(P, lx, ly, lz, hx, hy, hz, t_lo, t_hi, tn, tf) ? tn : INFINITY;
+  return fmaxf(tn, 0.f);
 }
 
 // Breadth-first walk: the leaf keys (entry bound bits << 32 | position) of every leaf the
-// packet can meet at some t in [t_lo, t_hi], into cand[0, n). Returns n, or -1 when a
-// level or the leaf list does not fit its shared-memory capacity.
-__device__ __noinline__ int packet_leaves(const Node* __restrict__ nodes, const PacketBounds& P, float t_lo,
-                                             float t_hi, int* front, uint64_t* cand, int lane) {
+// packet can meet, into cand[0, n). Returns n, or -1 when a level or the leaf list does
+// not fit its shared-memory capacity.
+__device__ __forceinline__ int packet_leaves(const Node* __restrict__ nodes, const PacketBounds& P, float cap,
+                                             int* front, uint64_t* cand, int lane) {
   int* cur = front;
   int* nxt = front + kFrontierCap;
   if (lane == 0) cur[0] = 0;
@@ -644,44 +628,34 @@ __device__ __noinline__ int packet_leaves(const Node* __restrict__ nodes, const 
   for (int level = 0; nf > 0; ++level) {
     if (level >= 4 * kStackDepth) return -1;  // deeper than any tree the build makes
     int nn = 0;
-    // two nodes per lane per batch: both loads are in flight before either box test
-    for (int base = 0; base < nf; base += 64) {
-      Node nd[2];
-      bool have[2];
-#pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        const int i = base + 32 * u + lane;
-        have[u] = i < nf;
-        if (have[u]) nd[u] = load_node(nodes, cur[i]);
+    for (int base = 0; base < nf; base += 32) {
+      const int i = base + lane;
+      float te0 = INFINITY, te1 = INFINITY;
+      int c0 = 0, c1 = 0;
+      if (i < nf) {
+        const Node nd = load_node(nodes, cur[i]);
+        te0 = packet_entry(P, nd.a.x, nd.a.y, nd.a.z, nd.a.w, nd.b.x, nd.b.y, cap);
+        te1 = packet_entry(P, nd.b.z, nd.b.w, nd.c.x, nd.c.y, nd.c.z, nd.c.w, cap);
+        c0 = nd.d.x;
+        c1 = nd.d.y;
       }
 #pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        float te0 = INFINITY, te1 = INFINITY;
-        int c0 = 0, c1 = 0;
-        if (have[u]) {
-          te0 = packet_entry(P, nd[u].a.x, nd[u].a.y, nd[u].a.z, nd[u].a.w, nd[u].b.x, nd[u].b.y, t_lo, t_hi);
-          te1 = packet_entry(P, nd[u].b.z, nd[u].b.w, nd[u].c.x, nd[u].c.y, nd[u].c.z, nd[u].c.w, t_lo, t_hi);
-          c0 = nd[u].d.x;
-          c1 = nd[u].d.y;
+      for (int k = 0; k < 2; ++k) {
+        const float te = k ? te1 : te0;
+        const int c = k ? c1 : c0;
+        const bool hit = te != INFINITY;
+        const unsigned mi = __ballot_sync(kFull, hit && c >= 0);
+        const unsigned ml = __ballot_sync(kFull, hit && c < 0);
+        if (hit && c >= 0) {
+          const int q = nn + __popc(mi & below);
+          if (q < kFrontierCap) nxt[q] = c;
         }
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-          const float te = k ? te1 : te0;
-          const int c = k ? c1 : c0;
-          const bool hit = te != INFINITY;
-          const unsigned mi = __ballot_sync(kFull, hit && c >= 0);
-          const unsigned ml = __ballot_sync(kFull, hit && c < 0);
-          if (hit && c >= 0) {
-            const int q = nn + __popc(mi & below);
-            if (q < kFrontierCap) nxt[q] = c;
-          }
-          if (hit && c < 0) {
-            const int q = nc + __popc(ml & below);
-            if (q < kCandCap) cand[q] = (uint64_t(__float_as_uint(te)) << 32) | uint32_t(~c);
-          }
-          nn += __popc(mi);
-          nc += __popc(ml);
+        if (hit && c < 0) {
+          const int q = nc + __popc(ml & below);
+          if (q < kCandCap) cand[q] = (uint64_t(__float_as_uint(te)) << 32) | uint32_t(~c);
         }
+        nn += __popc(mi);
+        nc += __popc(ml);
       }
     }
     __syncwarp();
@@ -694,199 +668,97 @@ __device__ __noinline__ int packet_leaves(const Node* __restrict__ nodes, const 
   return nc;
 }
 
-__device__ __forceinline__ uint64_t shfl_xor64(uint64_t v, int m) {
-  const uint32_t lo = __shfl_xor_sync(kFull, uint32_t(v), m), hi = __shfl_xor_sync(kFull, uint32_t(v >> 32), m);
-  return (uint64_t(hi) << 32) | lo;
-}
-
-// Ascending bitonic sort of 32 * E keys held E per lane (key lane * E + r in k[r]): the
-// stages whose partners lie in the same lane compare-swap registers, the others exchange
-// with lane ^ (stride / E) by shuffles. No shared memory, no warp barriers.
-template <int E>
-__device__ __forceinline__ void sort_regs(uint64_t (&k)[E], int lane) {
-#pragma unroll
-  for (int size = 2; size <= 32 * E; size <<= 1) {
-#pragma unroll
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      if (stride < E) {
-#pragma unroll
-        for (int r = 0; r < E; ++r) {
-          const int q = r ^ stride;
-          if (q > r) {
-            const bool up = ((lane * E + r) & size) == 0;
-            const uint64_t a = k[r], b = k[q];
-            const bool sw = (a > b) == up;
-            k[r] = sw ? b : a;
-            k[q] = sw ? a : b;
+// Ascending bitonic sort of cand[0, n) in shared memory by the warp (n <= kCandCap).
+__device__ __forceinline__ void sort_keys(uint64_t* cand, int n, int lane) {
+  int w = 32;
+  while (w < n) w <<= 1;
+  for (int i = n + lane; i < w; i += 32) cand[i] = kEmptyKey;
+  __syncwarp();
+  for (int k = 2; k <= w; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = lane; i < w; i += 32) {
+        const int l = i ^ j;
+        if (l > i) {
+          const uint64_t a = cand[i], b = cand[l];
+          if ((a > b) == ((i & k) == 0)) {
+            cand[i] = b;
+            cand[l] = a;
           }
         }
-      } else {
-        const int m = stride / E;
-        const bool lower = (lane & m) == 0;
-#pragma unroll
-        for (int r = 0; r < E; ++r) {
-          const uint64_t o = shfl_xor64(k[r], m);
-          const bool up = ((lane * E + r) & size) == 0;
-          const bool take_min = lower == up;
-          k[r] = take_min ? (o < k[r] ? o : k[r]) : (o > k[r] ? o : k[r]);
-        }
       }
+      __syncwarp();
     }
   }
-}
-
-// Sorts cand[0, n) ascending in place (n <= kCandCap = 32 * 16). Not inlined: one copy
-// per translation unit instead of one per kernel.
-template <int E>
-__device__ __noinline__ void sort_keys_e(uint64_t* cand, int n, int lane) {
-  uint64_t k[E];
-#pragma unroll
-  for (int r = 0; r < E; ++r) {
-    const int i = lane * E + r;
-    k[r] = i < n ? cand[i] : kEmptyKey;
-  }
-  sort_regs<E>(k, lane);
-  __syncwarp();
-#pragma unroll
-  for (int r = 0; r < E; ++r) cand[lane * E + r] = k[r];
-  __syncwarp();
-}
-
-__device__ __forceinline__ void sort_keys(uint64_t* cand, int n, int lane) {
-  if (n <= 32 * 4) sort_keys_e<4>(cand, n, lane);
-  else if (n <= 32 * 8) sort_keys_e<8>(cand, n, lane);
-  else sort_keys_e<16>(cand, n, lane);
 }
 
 // The frustum phase of a warp's packet. Returns whether this lane's ray still needs rounds
 // (L then holds its state after its last integrated event, L.lower that event's key).
-//
-// It runs in stages over consecutive t ranges [lo, hi): a stage lists and integrates the
-// leaves the packet can meet in its range; every event below hi is then final, the buffer
-// is dropped, and the next stage starts at hi, taking only events after the last
-// integrated one (L.lower). A range whose lists overflow shared memory is halved and
-// walked again. The first stage covers kFirstStage of the packet's t extent in the scene.
-//
-// Not inlined: one copy per buffer size and SH degree instead of one in every kernel; the
-// ray and its loop state are copied into registers once per packet, the scene and launch
-// constants are read through their references.
 template <int KBUF, int DEG>
-__device__ __noinline__ bool frustum_phase(const SceneRef& sc, const TraceCtx& C, const Ray& ray0, const float* B,
-                                           int bs, int64_t slot, int64_t r, int* wsm, int lane, bool act,
-                                           RayLoop& L0) {
+__device__ __forceinline__ bool frustum_phase(const SceneRef& sc, const TraceCtx& C, const Ray& ray, const float* B,
+                                              int bs, int64_t slot, int64_t r, int* wsm, int lane, bool act,
+                                              RayLoop& L) {
   if (!__any_sync(kFull, act)) return act;
-  const Ray ray = ray0;
-  RayLoop L = L0;
   const RaySlab sl = make_slab(ray);
-  const float cap = fminf(C.tmax, kSentinel);
-  PacketBounds P = packet_bounds(ray, sl, act);
-  // the packet's t extent in the scene box (the union of the root's child boxes): no event of
-  // a packet ray lies beyond `end`
-  float end = -INFINITY;
-  {
-    const Node root = load_node(sc.nodes, 0);
-    float tn, tf;
-    if (packet_span(P, root.a.x, root.a.y, root.a.z, root.a.w, root.b.x, root.b.y, 0.f, cap, tn, tf))
-      end = fmaxf(end, tf);
-    if (packet_span(P, root.b.z, root.b.w, root.c.x, root.c.y, root.c.z, root.c.w, 0.f, cap, tn, tf))
-      end = fmaxf(end, tf);
-    end = fminf(end, cap);
+  float cap = fminf(C.tmax, kSentinel);
+  // With a depth hint the walk covers t up to the packet's largest guessed stopping t (plus
+  // 5%): events up to there are integrated here, the rounds continue any ray that goes on.
+  // A poor guess costs time, never correctness.
+  float t_final = INFINITY;
+  if (C.depth_hint) {
+    const float h = warp_max(act ? C.depth_hint[r] : -INFINITY);
+    if (h > 0.f && 1.05f * h + 1e-3f < cap) cap = t_final = 1.05f * h + 1e-3f;
   }
+  const PacketBounds P = packet_bounds(ray, sl, act);
   int* front = wsm + kStackDepth;
   uint64_t* cand = reinterpret_cast<uint64_t*>(front + 2 * kFrontierCap);
-  // the bounds wait in shared memory while the leaves are integrated (registers are scarce)
-  PacketBounds* saved = reinterpret_cast<PacketBounds*>(cand + kCandCap);
-  if (lane == 0) *saved = P;
-  __syncwarp();
+  const int nc = packet_leaves(sc.nodes, P, cap, front, cand, lane);
+  if (nc < 0) return act;  // lists too long for shared memory: the rounds trace the packet
+  sort_keys(cand, nc, lane);
+  uint64_t buf[KBUF];
+#pragma unroll
+  for (int i = 0; i < KBUF; ++i) buf[i] = kEmptyKey;
   bool live = act;  // still integrating in this phase
-  float lo = 0.f;
-  float span = kFirstStage * fmaxf(end - lo, 0.f);
-  if (C.depth_hint) {
-    // the first stage reaches the packet's largest guessed stopping t (plus 5%); a ray that
-    // goes on continues in the next stage, so a poor guess costs time, never correctness
-    const float h = warp_max(act ? C.depth_hint[r] : -INFINITY);
-    if (h > 0.f && h < INFINITY) span = fminf(span, 1.05f * h + 1e-3f);
-  }
-  int walks = 0;
-  for (int tries = 0; end >= 0.f && __any_sync(kFull, live);) {
-    // bounded: at most kMaxWalks walks, and every stage must advance lo in float;
-    // otherwise the rounds trace what is left
-    if (++walks > kMaxWalks) break;
-    const bool last = !(lo + span < end);
-    const float hi = last ? end : lo + span;
-    if (!last && !(hi > lo)) break;
-    const int nc = packet_leaves(sc.nodes, *saved, lo, hi, front, cand, lane);
-    if (nc < 0) {  // too many nodes or leaves in this range: halve it
-      if (++tries > kMaxHalvings) break;  // the rounds trace what is left
-      span *= 0.5f;
-      continue;
+  for (int ci = 0;; ++ci) {
+    // every 32 leaves, the lanes start the loads of the next 32 records into L1 (one each),
+    // so the broadcast record loads of the loop below rarely wait on L2
+    if ((ci & 31) == 0 && ci + lane < nc)
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(sc.recs + int(uint32_t(cand[ci + lane]))));
+    const uint64_t ck = ci < nc ? cand[ci] : kEmptyKey;
+    const float T = ci < nc ? key_t(ck) : t_final;
+    // events below T are final: no leaf still to come has an event before T
+    while (live && buf[0] != kEmptyKey && key_t(buf[0]) < T) {
+      const uint64_t k = buf[0];
+#pragma unroll
+      for (int i = 0; i < KBUF - 1; ++i) buf[i] = buf[i + 1];
+      buf[KBUF - 1] = kEmptyKey;
+      L.lower = k;
+      if (consume_event<DEG>(sc, C, ray, B, bs, slot, k, L.s, L.last_dirac, L.iters, L.s16, L.cnt16, L.status)) {
+        live = false;
+        act = false;  // finished
+      }
     }
-    sort_keys(cand, nc, lane);
-    uint64_t buf[KBUF];
-#pragma unroll
-    for (int i = 0; i < KBUF; ++i) buf[i] = kEmptyKey;
-    const float t_final = last ? INFINITY : hi;
-    for (int cb = 0;; cb += kLeafGroup) {
-      // every 32 leaves, the lanes start the loads of the next 32 records into L1 (one
-      // each), so the broadcast record loads below rarely wait on L2
-      if ((cb & 31) == 0 && cb + lane < nc)
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(sc.recs + int(uint32_t(cand[cb + lane]))));
-      // events below T are final: no leaf still to come has an event before T. They are
-      // integrated once per group of leaves, when the lanes have several at once.
-      const float T = cb < nc ? key_t(cand[cb]) : t_final;
-      while (live && buf[0] != kEmptyKey && key_t(buf[0]) < T) {
-        const uint64_t k = buf[0];
-#pragma unroll
-        for (int i = 0; i < KBUF - 1; ++i) buf[i] = buf[i + 1];
-        buf[KBUF - 1] = kEmptyKey;
-        L.lower = k;
-        if (consume_event<DEG>(sc, C, ray, B, bs, slot, k, L.s, L.last_dirac, L.iters, L.s16, L.cnt16, L.status)) {
+    if (ci >= nc) break;
+    if (!__any_sync(kFull, live)) break;
+    if (live) {
+      const int j = int(uint32_t(ck));
+      const Record R = load_record(sc.recs, j);
+      HitT H;
+      if (intersect(R, ray, H)) {
+        const bool in0 = H.t0 > L.s16 && H.t0 <= C.tmax;
+        const bool in1 = H.t1 > L.s16 && (H.t1 <= C.tmax || in0);
+        // a full buffer cannot take another event: stop here, the rounds continue the ray
+        if ((in0 || in1) && buf[KBUF - (in0 && in1 ? 2 : 1)] != kEmptyKey) {
           live = false;
-          act = false;  // finished
-        }
-      }
-      if (cb >= nc) break;
-      if (!__any_sync(kFull, live)) break;
-      // the group's leaves: independent tests (their loads and roots overlap), then inserts
-      uint64_t e0[kLeafGroup], e1[kLeafGroup];
-#pragma unroll
-      for (int g = 0; g < kLeafGroup; ++g) {
-        e0[g] = e1[g] = kEmptyKey;
-        if (live && cb + g < nc) {
-          const int j = int(uint32_t(cand[cb + g]));
-          HitT H;
-          if (intersect(load_record(sc.recs, j), ray, H)) {
-            const bool in0 = H.t0 > L.s16 && H.t0 <= C.tmax;
-            if (in0) e0[g] = event_key(H.t0, j, 0);
-            if (H.t1 > L.s16 && (H.t1 <= C.tmax || in0)) e1[g] = event_key(H.t1, j, 1);
-          }
-        }
-      }
-#pragma unroll
-      for (int g = 0; g < kLeafGroup; ++g) {
-#pragma unroll
-        for (int x = 0; x < 2; ++x) {
-          const uint64_t e = x ? e1[g] : e0[g];
-          // earlier stages integrated everything up to L.lower
-          if (live && e != kEmptyKey && e > L.lower) {
-            // a full buffer cannot take another event: stop here, the rounds continue the ray
-            if (buf[KBUF - 1] != kEmptyKey) live = false;
-            else buf_insert(buf, e);
-          }
+        } else {
+          if (in0) buf_insert(buf, event_key(H.t0, j, 0));
+          if (in1) buf_insert(buf, event_key(H.t1, j, 1));
         }
       }
     }
-    if (last) {
-      // every stage done and every event integrated: nothing is left on a lane still active
-      if (live) act = false;
-      break;
-    }
-    lo = hi;
-    span = fminf(2.f * span, end - lo);  // the next range may be wider again
-    tries = 0;
   }
-  if (end < 0.f) act = false;  // the packet misses the scene: no events at all
-  L0 = L;
+  // all leaves taken and every event integrated: nothing is left on a lane still active,
+  // unless the walk stopped short of the scene (depth hint)
+  if (live && t_final == INFINITY) act = false;
   return act;
 }
 

@@ -3,15 +3,16 @@ and bench.py's CPU baseline, never by the product path).
 
 The network has no counterpart in the reference. Its specification is the GPU kernel's:
 - input: 39 features of the point of the ray's line closest to the scene centre, zero-padded
-  to 64 columns, rounded to bf16;
+  to 64 columns (the kernel reads 48; columns 39.. are zero), rounded to bf16;
 - layers: z1 = A0 W1^T + b1, A1 = bf16(relu(z1)); z2 = A1 W2^T + b2, A2 = bf16(relu(z2));
   y = A2 W3^T + b3 (outputs 0 and 1 of 16);
 - weights are the bf16 roundings of the fp32 parameters; products are summed in fp64 here
   and rounded to fp32 before the fp32 bias add, as the tensor cores accumulate in fp32;
 - loss: mean over the batch of w0 (y0 - t0)^2 + w1 (y1 - t1)^2;
 - backward: G3 = bf16(dL/dy); dA2 = G3 W3, masked by A2 > 0, G2 = bf16(.); dA1 = G2 W2,
-  masked by A1 > 0, G1 = bf16(.). Weight gradients are G^T A from the bf16 operands; bias
-  gradients are batch sums of the unrounded (fp32) masked gradients.
+  masked by A1 > 0, G1 = bf16(.). Weight gradients are G^T A from the bf16 operands; the
+  hidden layers' bias gradients are batch sums of the same bf16 G1, G2 (the kernel forms
+  them as G^T 1 on the tensor cores), the output bias gradient the sum of the fp32 dL/dy.
 Parameter block layout (fp32): W1 [64x64], W2 [64x64], W3 [16x64], b1 [64], b2 [64], b3 [16].
 """
 from __future__ import annotations
@@ -58,7 +59,7 @@ def encode(rayo, rayd, centre=(0.0, 0.0, 0.0), inv_scale=1.0):
         arg = (s * x).astype(np.float64)
         cols += [np.sin(np.pi * arg[:, i]).astype(f32) for i in range(3)]
         cols += [np.cos(np.pi * arg[:, i]).astype(f32) for i in range(3)]
-    feat = np.zeros((x.shape[0], IN), f32)
+    feat = np.zeros((x.shape[0], IN), f32)  # columns FEAT.. stay zero
     feat[:, :FEAT] = np.stack(cols, 1)
     return feat
 
@@ -76,6 +77,8 @@ def forward(params, feat, rounding=True):
     P = unpack(params, np.float32 if rounding else np.float64)
     w1, w2, w3 = rnd(P["w1"]), rnd(P["w2"]), rnd(P["w3"])
     d = np.float64
+    feat = np.array(feat, copy=True)
+    feat[:, FEAT:] = 0  # the kernel reads the 39 features only
     a0 = rnd(feat)
     a1 = rnd(np.maximum(acc(a0.astype(d) @ w1.astype(d).T) + P["b1"], 0))
     a2 = rnd(np.maximum(acc(a1.astype(d) @ w2.astype(d).T) + P["b2"], 0))
@@ -114,7 +117,7 @@ def gradients(params, feat, target, w0=1.0, w1=1.0, rounding=True):
     gw1 = G1.astype(d).T @ F["a0"].astype(d)
     gw2 = G2.astype(d).T @ F["a1"].astype(d)
     gw3 = G3.astype(d).T @ F["a2"].astype(d)
-    grads = np.concatenate([gw1.ravel(), gw2.ravel(), gw3.ravel(), g1.astype(d).sum(0), g2.astype(d).sum(0),
+    grads = np.concatenate([gw1.ravel(), gw2.ravel(), gw3.ravel(), G1.astype(d).sum(0), G2.astype(d).sum(0),
                             g.astype(d).sum(0)])
     return grads, loss
 
