@@ -8,14 +8,17 @@
 // layer's K; the parameter block keeps W1 64 wide, its columns 39.. are padding). Outputs:
 // the cost the tracer logs per ray, [log(1 + consumed events), depth offset / scale].
 //
-// One persistent CTA per SM, warp-specialised:
+// One persistent CTA per SM:
 // - kWorkers worker warpgroups. Each takes its own tiles of 128 rays (the MMA's M): it
 //   encodes a tile into shared memory, and after each layer's MMAs reads the accumulator
 //   from tensor memory (bias, ReLU, bf16) into the next layer's operand tile. The rays of
 //   its next tile are loaded into registers while the current tile's MMAs run.
-// - one MMA warp. One thread issues every tcgen05.mma of the CTA: it serves the workers'
-//   requests in a fixed round-robin order, each request one layer (or one backward step)
-//   of one tile, and tcgen05.commit signals that worker's completion barrier.
+// - inference: one elected thread of each warpgroup issues that warpgroup's MMAs, so the
+//   warpgroups run unsynchronised and one's epilogue overlaps another's MMAs.
+// - training: one more warp, the MMA warp. Its one thread issues every tcgen05.mma of the
+//   CTA, serving the workers' requests (one layer or backward step of one tile each) in a
+//   fixed round-robin order, so the gradient sums over the tiles have a fixed order;
+//   tcgen05.commit signals the worker's completion barrier.
 // The workers' CUDA-core work (encoding, epilogues) overlaps the other workers' MMAs.
 // Operands live in shared memory in the canonical no-swizzle layouts: 8 x 8 bf16 core
 // matrices of 128 contiguous bytes. Activation tiles [ray][unit] are K-major operands of
@@ -94,13 +97,16 @@ __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence:
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
+// Potentially blocking test: the thread may sleep until the phase completes or about 0.1 ms
+// (the suspend-time hint, in ns) has passed, so waiting threads leave the issue slots to
+// the others instead of spinning.
 __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t phase) {
   uint32_t ok;
   asm volatile(
-      "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
       "selp.b32 %0, 1, 0, P1;\n\t}"
       : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(phase)
+      : "r"(smem_u32(bar)), "r"(phase), "r"(100000u)
       : "memory");
   return ok != 0;
 }
@@ -123,19 +129,6 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
 // Barrier among the 128 threads of one worker warpgroup (ids 1.. ; 0 is __syncthreads).
 __device__ __forceinline__ void worker_sync(int w) {
   asm volatile("bar.sync %0, 128;" ::"r"(w + 1) : "memory");
-}
-
-// True on every thread of worker w iff `v` holds on all of them (a barrier with an AND
-// reduction), so the warpgroup leaves its loop together.
-__device__ __forceinline__ bool worker_and(int w, bool v) {
-  uint32_t r;
-  asm volatile(
-      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.and.pred p, %2, 128, q;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(r)
-      : "r"(uint32_t(v)), "r"(w + 1)
-      : "memory");
-  return r != 0;
 }
 
 constexpr long long kWaitClocks = 1ll << 31;  // about a second
@@ -321,6 +314,7 @@ struct Smem {
   float gb3[kMmaWarp][2], loss[kMmaWarp];  // per worker-warp sums (fixed order)
   uint64_t ready[kWorkers], done[kWorkers];
   int quit[kWorkers];
+  int wfail[kWorkers];  // a wait of worker w ran out: its warpgroup stops at its next barrier
   int abort;   // the MMA warp gave up
   int failed;  // a wait of this CTA ran out
   uint32_t tmem_base;
@@ -347,10 +341,83 @@ __device__ __forceinline__ RayIn load_ray(const MlpParams& P, int64_t s) {
   return x;
 }
 
+// Threads of a CTA: the worker warpgroups, and for training the MMA warp.
+template <bool TRAIN>
+__host__ __device__ constexpr int threads_of() {
+  return TRAIN ? kThreads : 32 * kMmaWarp;
+}
+
+// Which accumulators of the CTA's weight and bias gradients hold a sum already (the first
+// MMA into each overwrites).
+struct GradStarted {
+  bool w3 = false, w2 = false, w1 = false;
+};
+
+// The MMAs of step q of worker w's current tile, issued by one thread:
+// 0-2 the layers; training 3 dA2 (+ dW3), 4 dA1 (+ dW2, db2), 5 dW1, db1.
+template <bool TRAIN>
+__device__ __forceinline__ void issue_step(Smem<TRAIN>& S, uint32_t tmem, int w, int q, GradStarted& gs) {
+  const uint32_t sw1 = smem_u32(S.w1), sw2 = smem_u32(S.w2), sw3 = smem_u32(S.w3);
+  const uint32_t d = tmem + 64u * uint32_t(w);
+  const uint32_t sa0 = smem_u32(S.t[w].a0), sh1 = smem_u32(S.t[w].h1);
+  if (q == 0) {  // layer 1: D = A0 W1^T
+#pragma unroll
+    for (int ks = 0; ks < kK0 / 16; ++ks)
+      mma(d, desc_k(sa0, kTile, ks), desc_k(sw1, kHid, ks), idesc(128, kHid, false, false), ks > 0);
+    return;
+  }
+  if (q == 1) {  // layer 2: D = H1 W2^T
+#pragma unroll
+    for (int ks = 0; ks < kHid / 16; ++ks)
+      mma(d, desc_k(sh1, kTile, ks), desc_k(sw2, kHid, ks), idesc(128, kHid, false, false), ks > 0);
+    return;
+  }
+  if constexpr (!TRAIN) {  // layer 3: D[., 0:16] = H2 W3^T (inference keeps H2 in h1)
+#pragma unroll
+    for (int ks = 0; ks < kHid / 16; ++ks)
+      mma(d, desc_k(sh1, kTile, ks), desc_k(sw3, kOut, ks), idesc(128, kOut, false, false), ks > 0);
+  } else {
+    const uint32_t sh2 = smem_u32(S.t[w].h2), sg3 = smem_u32(S.t[w].g3), sones = smem_u32(S.ones);
+    if (q == 2) {  // layer 3
+      for (int ks = 0; ks < kHid / 16; ++ks)
+        mma(d, desc_k(sh2, kTile, ks), desc_k(sw3, kOut, ks), idesc(128, kOut, false, false), ks > 0);
+    } else if (q == 3) {
+      // dA2[128 x 64] = G3[128 x 16] W3[16 x 64] (W3 read MN-major: MN = h2, K = out)
+      mma(d, desc_k(sg3, kTile, 0), desc_mn(sw3, kOut, 0), idesc(128, kHid, false, true), 0);
+      // dW3^T[h2][out] += A2^T G3 (both tiles MN-major, K = ray)
+      for (int ks = 0; ks < kTile / 16; ++ks)
+        mma(tmem + kColGW3, desc_mn(sh2, kTile, ks), desc_mn(sg3, kTile, ks), idesc(64, kOut, true, true),
+            uint32_t(ks > 0 || gs.w3));
+      gs.w3 = true;
+    } else if (q == 4) {
+      // dA1 = G2 W2 (W2 MN-major: MN = h1, K = h2); G2 lives in h2
+      for (int ks = 0; ks < kHid / 16; ++ks)
+        mma(d, desc_k(sh2, kTile, ks), desc_mn(sw2, kHid, ks), idesc(128, kHid, false, true), ks > 0);
+      for (int ks = 0; ks < kTile / 16; ++ks) {
+        const uint32_t acc = uint32_t(ks > 0 || gs.w2);
+        // dW2[h2][h1] += G2^T A1
+        mma(tmem + kColGW2, desc_mn(sh2, kTile, ks), desc_mn(sh1, kTile, ks), idesc(64, kHid, true, true), acc);
+        // db2 (every column) += G2^T 1
+        mma(tmem + kColGB2, desc_mn(sh2, kTile, ks), desc_k(sones, kOnes, ks), idesc(64, kOnes, true, false), acc);
+      }
+      gs.w2 = true;
+    } else {
+      // G1 lives in h1: dW1[h1][0:48] += G1^T A0, db1 += G1^T 1
+      for (int ks = 0; ks < kTile / 16; ++ks) {
+        const uint32_t acc = uint32_t(ks > 0 || gs.w1);
+        mma(tmem + kColGW1, desc_mn(sh1, kTile, ks), desc_mn(sa0, kTile, ks), idesc(64, kK0, true, true), acc);
+        mma(tmem + kColGB1, desc_mn(sh1, kTile, ks), desc_k(sones, kOnes, ks), idesc(64, kOnes, true, false), acc);
+      }
+      gs.w1 = true;
+    }
+  }
+}
+
 // Inference (TRAIN = false: predictions and cost bins) or the gradients of one training
 // batch (TRAIN = true: each CTA writes its partial gradient and loss to P.partial).
 template <bool TRAIN>
-__global__ void __launch_bounds__(kThreads, 1) k_mlp(const MlpParams P) {
+__global__ void __launch_bounds__(threads_of<TRAIN>(), 1) k_mlp(const MlpParams P) {
+  constexpr int kThreadsT = threads_of<TRAIN>();
   extern __shared__ __align__(128) unsigned char smem_raw[];
   Smem<TRAIN>& S = *reinterpret_cast<Smem<TRAIN>*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -364,21 +431,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp(const MlpParams P) {
     const __nv_bfloat16* w1 = static_cast<const __nv_bfloat16*>(P.w1);
     const __nv_bfloat16* w2 = static_cast<const __nv_bfloat16*>(P.w2);
     const __nv_bfloat16* w3 = static_cast<const __nv_bfloat16*>(P.w3);
-    for (int i = tid; i < kHid * kK0 / 8; i += kThreads) {
+    for (int i = tid; i < kHid * kK0 / 8; i += kThreadsT) {
       const int o = i / (kK0 / 8), c0 = (i % (kK0 / 8)) * 8;
       *reinterpret_cast<uint4*>(S.w1 + kmaj(o, c0, kHid)) = *reinterpret_cast<const uint4*>(w1 + o * kIn + c0);
     }
-    for (int i = tid; i < kHid * kHid / 8; i += kThreads) {
+    for (int i = tid; i < kHid * kHid / 8; i += kThreadsT) {
       const int o = i / (kHid / 8), c0 = (i % (kHid / 8)) * 8;
       *reinterpret_cast<uint4*>(S.w2 + kmaj(o, c0, kHid)) = *reinterpret_cast<const uint4*>(w2 + o * kHid + c0);
     }
-    for (int i = tid; i < kOut * kHid / 8; i += kThreads) {
+    for (int i = tid; i < kOut * kHid / 8; i += kThreadsT) {
       const int o = i / (kHid / 8), c0 = (i % (kHid / 8)) * 8;
       *reinterpret_cast<uint4*>(S.w3 + kmaj(o, c0, kOut)) = *reinterpret_cast<const uint4*>(w3 + o * kHid + c0);
     }
     if (TRAIN) {
       const uint32_t one2 = 0x3F803F80u;  // two bf16 1.0
-      for (int i = tid; i < kOnes * kTile * 2 / 16; i += kThreads)
+      for (int i = tid; i < kOnes * kTile * 2 / 16; i += kThreadsT)
         reinterpret_cast<uint4*>(S.ones)[i] = make_uint4(one2, one2, one2, one2);
     }
   }
@@ -391,7 +458,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp(const MlpParams P) {
     S.gb3[tid][0] = S.gb3[tid][1] = 0.f;
     S.loss[tid] = 0.f;
   }
-  if (tid < kWorkers) S.quit[tid] = 0;
+  if (tid < kWorkers) S.quit[tid] = S.wfail[tid] = 0;
   if (tid == 0) {
     S.abort = 0;
     S.failed = 0;
@@ -401,7 +468,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp(const MlpParams P) {
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == kMmaWarp) {
+  // tensor memory: the MMA warp's (training) or the first worker warp's (inference)
+  constexpr int kAllocWarp = TRAIN ? kMmaWarp : 0;
+  if (warp == kAllocWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem_base)),
                  "r"(kCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -413,8 +482,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp(const MlpParams P) {
   const uint32_t tmem = S.tmem_base;
   bool ok = true;
 
-  if (warp == kMmaWarp) {
-    // ---- MMA warp: one thread serves the workers' requests in round-robin order
+  if (TRAIN && warp == kMmaWarp) {
+    // ---- MMA warp (training): one thread serves the workers' requests in round-robin
+    // order, so the gradient accumulators sum the tiles in a fixed order
     if (lane == 0) {
       int64_t left[kWorkers];
       uint32_t rphase[kWorkers];
@@ -427,8 +497,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp(const MlpParams P) {
         rphase[w] = 0;
         step[w] = 0;
       }
-      bool gw3_started = false, gw2_started = false, gw1_started = false;  // first MMA overwrites
-      const uint32_t sw1 = smem_u32(S.w1), sw2 = smem_u32(S.w2), sw3 = smem_u32(S.w3), sones = smem_u32(S.ones);
+      GradStarted gs;
       while (total > 0 && ok) {
         for (int w = 0; w < kWorkers && ok; ++w) {
           if (left[w] == 0) continue;
@@ -449,54 +518,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp(const MlpParams P) {
           }
           rphase[w] ^= 1u;
           tc_fence_after();
-          const uint32_t d = tmem + 64u * uint32_t(w);
-          const uint32_t sa0 = smem_u32(S.t[w].a0), sh1 = smem_u32(S.t[w].h1);
-          const int q = step[w];
-          if (q == 0) {  // layer 1: D = A0 W1^T
-            for (int ks = 0; ks < kK0 / 16; ++ks)
-              mma(d, desc_k(sa0, kTile, ks), desc_k(sw1, kHid, ks), idesc(128, kHid, false, false), ks > 0);
-          } else if (q == 1) {  // layer 2: D = H1 W2^T
-            for (int ks = 0; ks < kHid / 16; ++ks)
-              mma(d, desc_k(sh1, kTile, ks), desc_k(sw2, kHid, ks), idesc(128, kHid, false, false), ks > 0);
-          } else if (q == 2) {  // layer 3: D[., 0:16] = H2 W3^T (inference keeps H2 in h1)
-            const uint32_t sh2 = TRAIN ? smem_u32(reinterpret_cast<WorkerTiles<true>&>(S.t[w]).h2) : sh1;
-            for (int ks = 0; ks < kHid / 16; ++ks)
-              mma(d, desc_k(sh2, kTile, ks), desc_k(sw3, kOut, ks), idesc(128, kOut, false, false), ks > 0);
-          } else if (TRAIN) {
-            WorkerTiles<true>& T = reinterpret_cast<WorkerTiles<true>&>(S.t[w]);
-            const uint32_t sh2 = smem_u32(T.h2), sg3 = smem_u32(T.g3);
-            if (q == 3) {
-              // dA2[128 x 64] = G3[128 x 16] W3[16 x 64] (W3 read MN-major: MN = h2, K = out)
-              mma(d, desc_k(sg3, kTile, 0), desc_mn(sw3, kOut, 0), idesc(128, kHid, false, true), 0);
-              // dW3^T[h2][out] += A2^T G3 (both tiles MN-major, K = ray)
-              for (int ks = 0; ks < kTile / 16; ++ks)
-                mma(tmem + kColGW3, desc_mn(sh2, kTile, ks), desc_mn(sg3, kTile, ks), idesc(64, kOut, true, true),
-                    uint32_t(ks > 0 || gw3_started));
-              gw3_started = true;
-            } else if (q == 4) {
-              // dA1 = G2 W2 (W2 MN-major: MN = h1, K = h2); G2 lives in h2
-              for (int ks = 0; ks < kHid / 16; ++ks)
-                mma(d, desc_k(sh2, kTile, ks), desc_mn(sw2, kHid, ks), idesc(128, kHid, false, true), ks > 0);
-              for (int ks = 0; ks < kTile / 16; ++ks) {
-                const uint32_t acc = uint32_t(ks > 0 || gw2_started);
-                // dW2[h2][h1] += G2^T A1
-                mma(tmem + kColGW2, desc_mn(sh2, kTile, ks), desc_mn(sh1, kTile, ks), idesc(64, kHid, true, true), acc);
-                // db2 (every column) += G2^T 1
-                mma(tmem + kColGB2, desc_mn(sh2, kTile, ks), desc_k(sones, kOnes, ks), idesc(64, kOnes, true, false),
-                    acc);
-              }
-              gw2_started = true;
-            } else {
-              // G1 lives in h1: dW1[h1][0:48] += G1^T A0, db1 += G1^T 1
-              for (int ks = 0; ks < kTile / 16; ++ks) {
-                const uint32_t acc = uint32_t(ks > 0 || gw1_started);
-                mma(tmem + kColGW1, desc_mn(sh1, kTile, ks), desc_mn(sa0, kTile, ks), idesc(64, kK0, true, true), acc);
-                mma(tmem + kColGB1, desc_mn(sh1, kTile, ks), desc_k(sones, kOnes, ks), idesc(64, kOnes, true, false),
-                    acc);
-              }
-              gw1_started = true;
-            }
-          }
+          issue_step<TRAIN>(S, tmem, w, step[w], gs);
           mma_commit(&S.done[w]);
           step[w] = step[w] + 1 == kSteps ? 0 : step[w] + 1;
           --left[w];
@@ -521,24 +543,39 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp(const MlpParams P) {
     int64_t tile = int64_t(blockIdx.x) * kWorkers + g;
     RayIn next = load_ray(P, tile * kTile + row);
     bool first = true;
+    bool stop = false;  // the same on every thread of the warpgroup (read after its barriers)
+    GradStarted none;   // inference accumulates no gradients
 
-    // bounded wait for the next completion of this worker's MMAs; every thread of the
-    // warpgroup gets the same answer
-    auto await_mma = [&]() -> bool {
-      const bool got = mbar_wait(&S.done[g], dphase, wait_limit);
+    // bounded wait for the next completion of this worker's MMAs; a thread whose wait runs
+    // out flags the warpgroup, which stops at its next barrier
+    auto await_mma = [&]() {
+      if (!mbar_wait(&S.done[g], dphase, wait_limit)) *reinterpret_cast<volatile int*>(&S.wfail[g]) = 1;
       dphase ^= 1u;
       tc_fence_after();
-      return worker_and(g, got);
     };
-    // hand the operand tiles to the MMA warp
-    auto hand_over = [&]() {
+    // hand the operand tiles of step q over: inference issues the step's MMAs itself (one
+    // thread), training hands them to the MMA warp. False when the warpgroup must stop.
+    auto hand_over = [&](int q) -> bool {
       fence_async_smem();
       tc_fence_before();
       worker_sync(g);
-      if (row == 0) mbar_arrive(&S.ready[g]);
+      if (*reinterpret_cast<volatile int*>(&S.wfail[g])) {
+        stop = true;
+        return false;
+      }
+      if (row == 0) {
+        if constexpr (TRAIN) {
+          mbar_arrive(&S.ready[g]);
+        } else {
+          tc_fence_after();
+          issue_step<TRAIN>(S, tmem, g, q, none);
+          mma_commit(&S.done[g]);
+        }
+      }
+      return true;
     };
 
-    for (; tile < ntiles && ok; tile += stride) {
+    for (; tile < ntiles && !stop; tile += stride) {
       const int64_t s = tile * kTile + row;
       const bool valid = s < P.num_samples;
       const int64_t r = valid ? (P.sample_idx ? int64_t(__ldg(P.sample_idx + s)) : s) : 0;
@@ -558,7 +595,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp(const MlpParams P) {
         next = load_ray(P, (tile + stride) * kTile + row);  // in flight during this tile's MMAs
       }
       // training: the previous tile's weight-gradient MMAs read a0 and h1
-      if (TRAIN && !first && !(ok = await_mma())) break;
+      if (TRAIN && !first) await_mma();
       first = false;
 #pragma unroll
       for (int c = 0; c < kK0 / 8; ++c)
@@ -566,9 +603,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp(const MlpParams P) {
             make_uint4(enc[4 * c], enc[4 * c + 1], enc[4 * c + 2], enc[4 * c + 3]);
       // ---- layers 1 and 2: bias, ReLU, bf16 into the next operand tile
 #pragma unroll 1
-      for (int layer = 0; layer < 2 && ok; ++layer) {
-        hand_over();
-        if (!(ok = await_mma())) break;
+      for (int layer = 0; layer < 2; ++layer) {
+        if (!hand_over(layer)) break;
+        await_mma();
         const float* b = layer == 0 ? S.b1 : S.b2;
         unsigned char* dst = (TRAIN && layer == 1) ? reinterpret_cast<WorkerTiles<true>&>(T).h2 : T.h1;
 #pragma unroll
@@ -586,10 +623,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp(const MlpParams P) {
           for (int c = 0; c < 2; ++c) st16(dst, row, 32 * half + 16 * c, kTile, h + 8 * c);
         }
       }
-      if (!ok) break;
+      if (stop) break;
       // ---- layer 3
-      hand_over();
-      if (!(ok = await_mma())) break;
+      if (!hand_over(2)) break;
+      await_mma();
       float y2[2];
       tmem_ld<2>(dcol, y2);
       const float y0 = y2[0] + S.b3[0], y1 = y2[1] + S.b3[1];
@@ -622,9 +659,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp(const MlpParams P) {
       // ---- dA2 = G3 W3 (and dW3): G2 = dA2 masked by A2 > 0, written over A2;
       // then dA1 = G2 W2 (and dW2, db2): G1 = dA1 masked by A1 > 0, written over A1
 #pragma unroll 1
-      for (int back = 0; back < 2 && ok; ++back) {
-        hand_over();
-        if (!(ok = await_mma())) break;
+      for (int back = 0; back < 2; ++back) {
+        if (!hand_over(3 + back)) break;
+        await_mma();
         unsigned char* act = back == 0 ? TT.h2 : TT.h1;
 #pragma unroll
         for (int half = 0; half < 2; ++half) {
@@ -644,14 +681,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp(const MlpParams P) {
           for (int c = 0; c < 2; ++c) st16(act, row, 32 * half + 16 * c, kTile, h + 8 * c);
         }
       }
-      if (!ok) break;
+      if (stop) break;
       // ---- dW1, db1: handed over now, waited for before a0 / h1 are overwritten
-      hand_over();
+      if (!hand_over(5)) break;
     }
     // training: the last tile's weight-gradient MMAs
-    if (TRAIN && ok && !first) ok = await_mma();
-    if (!ok) {
-      atomicExch(P.error, 1);
+    if (TRAIN && !stop && !first) await_mma();
+    worker_sync(g);
+    if (*reinterpret_cast<volatile int*>(&S.wfail[g])) stop = true;
+    if (stop) {
+      if (row == 0) atomicExch(P.error, 1);
       *reinterpret_cast<volatile int*>(&S.failed) = 1;
       // let this worker's MMAs in flight finish (bounded, at the full limit) before TMEM is
       // freed, unless the MMA warp itself gave up
@@ -719,7 +758,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp(const MlpParams P) {
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (warp == kMmaWarp) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
+  if (warp == kAllocWarp)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
 }
 
 // Sum of the per-CTA partial gradients (and losses) in CTA order.
@@ -794,7 +834,7 @@ cudaError_t launch_mlp(const MlpParams& P, bool train, int grid, cudaStream_t st
   auto kern = train ? k_mlp<true> : k_mlp<false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
-  kern<<<grid, kThreads, smem, st>>>(P);
+  kern<<<grid, train ? threads_of<true>() : threads_of<false>(), smem, st>>>(P);
   return cudaGetLastError();
 }
 
