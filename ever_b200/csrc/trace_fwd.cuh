@@ -535,6 +535,10 @@ __device__ __forceinline__ bool run_rounds(const SceneRef& sc, const TraceCtx& C
 // A lane whose buffer would overflow, and every lane of a packet whose breadth-first
 // lists overflow shared memory, stops after its last integrated event; the rounds then
 // continue it from there (lower = that event's key), so the results do not depend on it.
+// Events a lane holds in the frustum phase. Fewer than the rounds' buffer: the phase's
+// buffer lives across the whole leaf loop, and 12 of 16 gave the shortest forward at 1M
+// ellipsoids / 1080p (5.90 ms; 16: 6.22, 8: 6.85, 24: 7.13 ms with spills).
+constexpr int frustum_buffer(int kbuf) { return kbuf == 16 ? 12 : kbuf; }
 constexpr int kFrontierCap = 384;  // nodes per breadth-first level
 constexpr int kCandCap = 512;      // leaves per packet (a power of two: the sort's width)
 // Shared ints per warp: the traversal stack, two frontier levels, the leaf keys (64-bit).
@@ -669,7 +673,7 @@ __device__ __forceinline__ int packet_leaves(const Node* __restrict__ nodes, con
 }
 
 // Ascending bitonic sort of cand[0, n) in shared memory by the warp (n <= kCandCap).
-__device__ __forceinline__ void sort_keys(uint64_t* cand, int n, int lane) {
+__device__ __forceinline__ void sort_keys_smem(uint64_t* cand, int n, int lane) {
   int w = 32;
   while (w < n) w <<= 1;
   for (int i = n + lane; i < w; i += 32) cand[i] = kEmptyKey;
@@ -691,12 +695,76 @@ __device__ __forceinline__ void sort_keys(uint64_t* cand, int n, int lane) {
   }
 }
 
+__device__ __forceinline__ uint64_t shfl_xor64(uint64_t v, int m) {
+  const uint32_t lo = __shfl_xor_sync(kFull, uint32_t(v), m), hi = __shfl_xor_sync(kFull, uint32_t(v >> 32), m);
+  return (uint64_t(hi) << 32) | lo;
+}
+
+// Ascending bitonic sort of 32 * E keys held E per lane (key lane * E + r in k[r]): the
+// stages whose partners lie in the same lane compare-swap registers, the others exchange
+// with lane ^ (stride / E) by shuffles. No shared memory, no warp barriers.
+template <int E>
+__device__ __forceinline__ void sort_regs(uint64_t (&k)[E], int lane) {
+#pragma unroll
+  for (int size = 2; size <= 32 * E; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      if (stride < E) {
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+          const int q = r ^ stride;
+          if (q > r) {
+            const bool up = ((lane * E + r) & size) == 0;
+            const uint64_t a = k[r], b = k[q];
+            const bool sw = (a > b) == up;
+            k[r] = sw ? b : a;
+            k[q] = sw ? a : b;
+          }
+        }
+      } else {
+        const int m = stride / E;
+        const bool lower = (lane & m) == 0;
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+          const uint64_t o = shfl_xor64(k[r], m);
+          const bool up = ((lane * E + r) & size) == 0;
+          const bool take_min = lower == up;
+          k[r] = take_min ? (o < k[r] ? o : k[r]) : (o > k[r] ? o : k[r]);
+        }
+      }
+    }
+  }
+}
+
+// Sorts cand[0, n) ascending (n <= 32 * E) through registers.
+template <int E>
+__device__ __forceinline__ void sort_keys_r(uint64_t* cand, int n, int lane) {
+  uint64_t k[E];
+#pragma unroll
+  for (int r = 0; r < E; ++r) {
+    const int i = lane * E + r;
+    k[r] = i < n ? cand[i] : kEmptyKey;
+  }
+  sort_regs<E>(k, lane);
+  __syncwarp();
+#pragma unroll
+  for (int r = 0; r < E; ++r) cand[lane * E + r] = k[r];
+  __syncwarp();
+}
+// Up to 256 keys sort in registers; longer lists in shared memory.
+__device__ __forceinline__ void sort_keys(uint64_t* cand, int n, int lane) {
+  if (n <= 32 * 4) sort_keys_r<4>(cand, n, lane);
+  else if (n <= 32 * 8) sort_keys_r<8>(cand, n, lane);
+  else sort_keys_smem(cand, n, lane);
+}
+
 // The frustum phase of a warp's packet. Returns whether this lane's ray still needs rounds
 // (L then holds its state after its last integrated event, L.lower that event's key).
 template <int KBUF, int DEG>
 __device__ __forceinline__ bool frustum_phase(const SceneRef& sc, const TraceCtx& C, const Ray& ray, const float* B,
                                               int bs, int64_t slot, int64_t r, int* wsm, int lane, bool act,
                                               RayLoop& L) {
+  constexpr int FBUF = frustum_buffer(KBUF);
   if (!__any_sync(kFull, act)) return act;
   const RaySlab sl = make_slab(ray);
   float cap = fminf(C.tmax, kSentinel);
@@ -714,9 +782,9 @@ __device__ __forceinline__ bool frustum_phase(const SceneRef& sc, const TraceCtx
   const int nc = packet_leaves(sc.nodes, P, cap, front, cand, lane);
   if (nc < 0) return act;  // lists too long for shared memory: the rounds trace the packet
   sort_keys(cand, nc, lane);
-  uint64_t buf[KBUF];
+  uint64_t buf[FBUF];
 #pragma unroll
-  for (int i = 0; i < KBUF; ++i) buf[i] = kEmptyKey;
+  for (int i = 0; i < FBUF; ++i) buf[i] = kEmptyKey;
   bool live = act;  // still integrating in this phase
   for (int ci = 0;; ++ci) {
     // every 32 leaves, the lanes start the loads of the next 32 records into L1 (one each),
@@ -729,8 +797,8 @@ __device__ __forceinline__ bool frustum_phase(const SceneRef& sc, const TraceCtx
     while (live && buf[0] != kEmptyKey && key_t(buf[0]) < T) {
       const uint64_t k = buf[0];
 #pragma unroll
-      for (int i = 0; i < KBUF - 1; ++i) buf[i] = buf[i + 1];
-      buf[KBUF - 1] = kEmptyKey;
+      for (int i = 0; i < FBUF - 1; ++i) buf[i] = buf[i + 1];
+      buf[FBUF - 1] = kEmptyKey;
       L.lower = k;
       if (consume_event<DEG>(sc, C, ray, B, bs, slot, k, L.s, L.last_dirac, L.iters, L.s16, L.cnt16, L.status)) {
         live = false;
@@ -747,7 +815,7 @@ __device__ __forceinline__ bool frustum_phase(const SceneRef& sc, const TraceCtx
         const bool in0 = H.t0 > L.s16 && H.t0 <= C.tmax;
         const bool in1 = H.t1 > L.s16 && (H.t1 <= C.tmax || in0);
         // a full buffer cannot take another event: stop here, the rounds continue the ray
-        if ((in0 || in1) && buf[KBUF - (in0 && in1 ? 2 : 1)] != kEmptyKey) {
+        if ((in0 || in1) && buf[FBUF - (in0 && in1 ? 2 : 1)] != kEmptyKey) {
           live = false;
         } else {
           if (in0) buf_insert(buf, event_key(H.t0, j, 0));
