@@ -80,7 +80,7 @@ class BatchedTracer:
         self.iters = torch.empty(R, dtype=torch.int32, device=dev)
         self.ray_stats = torch.empty((R, 2), **f32)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
-        self.event_log = torch.empty((self.max_iters, self.num_slots), dtype=torch.int32, device=dev)
+        self.event_log = torch.empty((self.num_slots, self.max_iters), dtype=torch.int32, device=dev)
         self.grad_out = torch.zeros((R, 5), **f32)
         self.drayo = torch.empty((R, 3), **f32)
         self.drayd = torch.empty((R, 3), **f32)

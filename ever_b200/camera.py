@@ -136,7 +136,7 @@ def forward(scene: T.Scene, camera: Camera, jitter=None, tmin=0.0, tmax=1000.0, 
     res = T.ForwardResult(
         out=torch.empty((R, 5), **f32), states=torch.empty((R, 16), **f32), last_dirac=torch.empty((R, 4), **f32),
         iters=torch.empty(R, dtype=torch.int32, device=device),
-        event_log=(torch.empty((max(int(max_iters), 0), S), dtype=torch.int32, device=device)
+        event_log=(torch.empty((S, max(int(max_iters), 0)), dtype=torch.int32, device=device)
                    if log_events else None),
         touch_count=(torch.zeros(scene.num_prims, dtype=torch.int32, device=device) if touch_count else None),
         ray_stats=(torch.empty((R, 2), **f32) if ray_stats else None),
@@ -144,7 +144,7 @@ def forward(scene: T.Scene, camera: Camera, jitter=None, tmin=0.0, tmax=1000.0, 
     o = N.EverForwardOut()
     o.out, o.states, o.last_dirac, o.iters = N.ptr(res.out), N.ptr(res.states), N.ptr(res.last_dirac), N.ptr(res.iters)
     o.event_log = N.ptr(res.event_log)
-    o.log_cap = 0 if res.event_log is None else res.event_log.shape[0]
+    o.log_cap = 0 if res.event_log is None else res.event_log.shape[1]
     o.touch_count = N.ptr(res.touch_count)
     o.ray_stats = N.ptr(res.ray_stats)
     o.status = N.ptr(res.status)
@@ -214,7 +214,7 @@ def backward(scene: T.Scene, camera: Camera, fwd: T.ForwardResult, grad_out, jit
     with torch.cuda.device(device):
         N.check(lib.ever_trace_backward_camera(
             ctypes.byref(scene.c), ctypes.byref(camera.c()), N.ptr(jitter), ctypes.byref(args), N.ptr(grad_out),
-            N.ptr(fwd.states), N.ptr(fwd.iters), N.ptr(fwd.event_log), fwd.event_log.shape[0], N.ptr(wct), num_wct,
+            N.ptr(fwd.states), N.ptr(fwd.iters), N.ptr(fwd.event_log), fwd.event_log.shape[1], N.ptr(wct), num_wct,
             N.ptr(m), N.ptr(s), N.ptr(q), N.ptr(ws), int(ws.numel()), N.ptr(slot_order),
             ctypes.byref((tune or T.Tune()).c()), ctypes.byref(o), _stream(device)))
     return g
@@ -229,7 +229,7 @@ def tri_collection(scene: T.Scene, camera: Camera, fwd: T.ForwardResult, max_ite
     tri = torch.empty(R * int(max_iters), dtype=torch.int32, device=scene.device)
     with torch.cuda.device(scene.device):
         N.check(N.load().ever_camera_event_log_to_reference(ctypes.byref(scene.c), ctypes.byref(camera.c()),
-                                                            N.ptr(log), log.shape[0], N.ptr(fwd.iters), N.ptr(tri),
+                                                            N.ptr(log), log.shape[1], N.ptr(fwd.iters), N.ptr(tri),
                                                             int(max_iters), _stream(scene.device)))
     return tri
 

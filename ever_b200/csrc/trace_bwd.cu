@@ -243,8 +243,8 @@ struct BRayCtx {
   const float* grad_out;
   const float* states;
   const int32_t* iters;
-  const int32_t* event_log;
-  int64_t log_stride;
+  const int32_t* event_log;  // ray-major: row `slot` holds the ray's event ids in order
+  int64_t log_cap;
   float* drayo;
   float* drayd;
   const float* wct;
@@ -463,11 +463,11 @@ __device__ void backward_ray(const BScene& S, const BRayCtx& P, int64_t r, int64
   float acc[kPendingSlots][kGradRow];
 #pragma unroll
   for (int q = 0; q < kPendingSlots; ++q) pj[q] = -1;
-  Ctrl cur = load_ctrl<DEG>(recs, S.features, fstride, ray, B, P.event_log[int64_t(n - 1) * P.log_stride + slot]);
+  Ctrl cur = load_ctrl<DEG>(recs, S.features, fstride, ray, B, P.event_log[slot * P.log_cap + (n - 1)]);
   for (int i = n - 1; i >= 0; --i) {
     Ctrl old;
     if (i > 0) {
-      old = load_ctrl<DEG>(recs, S.features, fstride, ray, B, P.event_log[int64_t(i - 1) * P.log_stride + slot]);
+      old = load_ctrl<DEG>(recs, S.features, fstride, ray, B, P.event_log[slot * P.log_cap + (i - 1)]);
     } else {
       old.t = 0.f;
       old.dirac = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -651,7 +651,7 @@ __global__ void __launch_bounds__(256, 2) k_trace_bwd(const BwdParams P) {
   const int64_t r = P.ray_order ? int64_t(P.ray_order[slot]) : slot;
   const BScene S{reinterpret_cast<const Node*>(P.nodes), reinterpret_cast<const Record*>(P.records), P.features,
                  P.order, P.K, P.acc_geo, P.acc_feat};
-  const BRayCtx C{P.rayo, P.rayd, P.tmin, P.max_iters, P.grad_out, P.states, P.iters, P.event_log, P.R,
+  const BRayCtx C{P.rayo, P.rayd, P.tmin, P.max_iters, P.grad_out, P.states, P.iters, P.event_log, P.log_cap,
                   P.drayo, P.drayd, P.wct, P.num_wct, P.dmeans2d};
   backward_ray<DEG>(S, C, r, slot, load3(P.rayo, r), load3(P.rayd, r));
 }
@@ -669,7 +669,7 @@ __global__ void __launch_bounds__(256, 2)
   if (p < 0) return;
   const BScene S{reinterpret_cast<const Node*>(P.nodes), reinterpret_cast<const Record*>(P.records), P.features,
                  P.order, P.K, P.acc_geo, P.acc_feat};
-  const BRayCtx C{nullptr, nullptr, P.tmin, P.max_iters, P.grad_out, P.states, P.iters, P.event_log, P.R,
+  const BRayCtx C{nullptr, nullptr, P.tmin, P.max_iters, P.grad_out, P.states, P.iters, P.event_log, P.log_cap,
                   P.drayo, P.drayd, P.wct, P.num_wct, P.dmeans2d};
   float3 ro, rd;
   camera_ray(cam, jitter, p, ro, rd);
@@ -683,7 +683,7 @@ __global__ void __launch_bounds__(256, 2)
 template <int DEG>
 __global__ void __launch_bounds__(256, 2) k_trace_bwd_batched(const BatchBwdParams P) {
   const int tid = threadIdx.x, lane = tid & 31;
-  const BRayCtx C{P.rayo, P.rayd, P.tmin, P.max_iters, P.grad_out, P.states, P.iters, P.event_log, P.num_slots,
+  const BRayCtx C{P.rayo, P.rayd, P.tmin, P.max_iters, P.grad_out, P.states, P.iters, P.event_log, P.log_cap,
                   P.drayo, P.drayd, nullptr, 0, nullptr};
   const int64_t num_packets = P.num_slots / 32;
   for (;;) {
@@ -798,7 +798,7 @@ __global__ void k_finalize_features(const int32_t* __restrict__ order, int64_t N
   }
 }
 
-// tri[i * R + ray] from log[i * R + slot], ray = ray_order[slot] (or slot).
+// tri[i * R + ray] from log[slot * log_cap + i], ray = ray_order[slot] (or slot).
 __global__ void k_log_to_reference(const int32_t* __restrict__ order, const int32_t* __restrict__ log, int log_cap,
                                    const int32_t* __restrict__ iters, int64_t R, const int32_t* __restrict__ ray_order,
                                    int32_t* __restrict__ tri, int max_iters) {
@@ -808,7 +808,7 @@ __global__ void k_log_to_reference(const int32_t* __restrict__ order, const int3
   const int64_t r = ray_order ? int64_t(ray_order[slot]) : slot;
   int32_t v = 0;
   if (i < iters[r] && i < log_cap) {
-    const int32_t id = log[i * R + slot];
+    const int32_t id = log[slot * log_cap + i];
     v = 2 * order[id >> 1] + (id & 1);
   }
   tri[i * R + r] = v;
@@ -844,7 +844,7 @@ __global__ void k_camera_log_to_reference(const CameraParams cam, int64_t num_sl
   if (r < 0) return;
   int32_t v = 0;
   if (i < iters[r] && i < log_cap) {
-    const int32_t id = log[i * num_slots + slot];
+    const int32_t id = log[slot * log_cap + i];
     v = 2 * order[id >> 1] + (id & 1);
   }
   tri[i * (int64_t(cam.width) * cam.height) + r] = v;

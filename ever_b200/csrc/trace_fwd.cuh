@@ -292,7 +292,6 @@ struct SceneRef {
 struct TraceCtx {
   float tmin, tmax;
   int max_iters;
-  int64_t log_stride;  // event-log row length (slots)
   EverForwardOut out;
   bool frustum;        // packet kernels: run the frustum phase before the rounds
   int depth;           // traversal stack entries in use (<= kStackDepth)
@@ -325,7 +324,7 @@ __device__ __forceinline__ bool consume_event(const SceneRef& sc, const TraceCtx
   last_dirac = dirac;
   if (C.out.event_log) {
     if (iters < C.out.log_cap)
-      C.out.event_log[int64_t(iters) * C.log_stride + slot] = 2 * j + (ex ? 0 : 1);
+      C.out.event_log[slot * int64_t(C.out.log_cap) + iters] = 2 * j + (ex ? 0 : 1);
     else
       status |= EVER_STATUS_LOG_OVERFLOW;
   }
@@ -426,7 +425,7 @@ __global__ void __launch_bounds__(256) k_trace_fwd_ray(const FwdParams P) {
   if (gi >= P.R) return;
   const int64_t r = P.ray_order ? int64_t(P.ray_order[gi]) : gi;
   const SceneRef sc = scene_of(P);
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out, P.frustum != 0, P.stack_depth, P.depth_hint};
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.out, P.frustum != 0, P.stack_depth, P.depth_hint};
   const Ray ray = load_ray(P.rayo, P.rayd, r, P.tmin);
   const RaySlab sl = make_slab(ray);
   float B[16];
@@ -896,7 +895,7 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value) k_trace_fwd
   const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;
   const bool valid = gi < P.R;  // every lane stays for the warp-wide ballots
   const int64_t r = valid ? (P.ray_order ? int64_t(P.ray_order[gi]) : gi) : 0;
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.R, P.out, P.frustum != 0, P.stack_depth, P.depth_hint};
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.out, P.frustum != 0, P.stack_depth, P.depth_hint};
   const Ray ray = load_ray(P.rayo, P.rayd, r, P.tmin);
   trace_packet<KBUF, DEG>(scene_of(P), C, ray, r, valid, gi, wstack, B, blockDim.x, lane);
 }
@@ -940,7 +939,7 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value)
   }
   if (!valid) r = 0;
   const SceneRef sc = scene_of(P);
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, slots, P.out, P.frustum != 0, P.stack_depth, P.depth_hint};
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.out, P.frustum != 0, P.stack_depth, P.depth_hint};
   Ray ray;
   if (CAM) {
     float3 ro, rd;
@@ -990,7 +989,7 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value)
   const int64_t gi = int64_t(blockIdx.x) * blockDim.x + tid;
   const int64_t p = gi < num_slots ? camera_slot_pixel(cam, gi) : -1;
   const bool valid = p >= 0;
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, num_slots, P.out, P.frustum != 0, P.stack_depth, P.depth_hint};
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.out, P.frustum != 0, P.stack_depth, P.depth_hint};
   float3 ro, rd;
   camera_ray(cam, jitter, valid ? p : 0, ro, rd);
   const Ray ray = make_ray(ro, rd, P.tmin);
@@ -1005,7 +1004,7 @@ __global__ void __launch_bounds__(BLOCK, FwdMinBlocks<BLOCK>::value) k_trace_fwd
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   int* wstack = smem + warp * kWarpInts;  // stack, then the frustum phase's lists
   float* B = reinterpret_cast<float*>(smem + (blockDim.x / 32) * kWarpInts) + tid;
-  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.num_slots, P.out, P.frustum != 0, P.stack_depth, nullptr};
+  const TraceCtx C{P.tmin, P.tmax, P.max_iters, P.out, P.frustum != 0, P.stack_depth, nullptr};
   const int64_t num_packets = P.num_slots / 32;
   for (;;) {
     unsigned int pk = 0;

@@ -121,7 +121,7 @@ class ForwardResult:
     states: torch.Tensor          # (R,16)
     last_dirac: torch.Tensor      # (R,4)
     iters: torch.Tensor           # (R,) int32
-    event_log: Optional[torch.Tensor]   # (log_cap, R) int32, Morton numbering
+    event_log: Optional[torch.Tensor]   # (R, log_cap) int32 ray-major (row = launch slot), Morton numbering
     touch_count: Optional[torch.Tensor] # (N,) int32
     ray_stats: Optional[torch.Tensor]   # (R,2)
     status: torch.Tensor          # (1,) int32
@@ -161,7 +161,7 @@ def forward(scene: Scene, rayo, rayd, tmin=0.0, tmax=1000.0, max_iters=500, sh_d
         buffers = ForwardResult(
             out=torch.empty((R, 5), **f32), states=torch.empty((R, 16), **f32),
             last_dirac=torch.empty((R, 4), **f32), iters=torch.empty(R, dtype=torch.int32, device=device),
-            event_log=(torch.empty((max(int(max_iters), 0), R), dtype=torch.int32, device=device)
+            event_log=(torch.empty((R, max(int(max_iters), 0)), dtype=torch.int32, device=device)
                        if log_events else None),
             touch_count=(torch.zeros(scene.num_prims, dtype=torch.int32, device=device) if touch_count else None),
             ray_stats=(torch.empty((R, 2), **f32) if ray_stats else None),
@@ -170,7 +170,7 @@ def forward(scene: Scene, rayo, rayd, tmin=0.0, tmax=1000.0, max_iters=500, sh_d
     o.out, o.states, o.last_dirac, o.iters = (N.ptr(buffers.out), N.ptr(buffers.states), N.ptr(buffers.last_dirac),
                                               N.ptr(buffers.iters))
     o.event_log = N.ptr(buffers.event_log)
-    o.log_cap = 0 if buffers.event_log is None else buffers.event_log.shape[0]
+    o.log_cap = 0 if buffers.event_log is None else buffers.event_log.shape[1]
     o.touch_count = N.ptr(buffers.touch_count)
     o.ray_stats = N.ptr(buffers.ray_stats)
     o.status = N.ptr(buffers.status)
@@ -243,7 +243,7 @@ def backward(scene: Scene, rayo, rayd, fwd: ForwardResult, grad_out, tmin=0.0, t
     o.dfeatures, o.drayo, o.drayd, o.dmeans2d = N.ptr(g.features), N.ptr(g.rayo), N.ptr(g.rayd), N.ptr(g.means2d)
     args = trace_args(tmin, tmax, max_iters, sh_degree)
     common = (ctypes.byref(scene.c), N.ptr(rayo), N.ptr(rayd), R, ctypes.byref(args), N.ptr(grad_out),
-              N.ptr(fwd.states), N.ptr(fwd.iters), N.ptr(fwd.event_log), fwd.event_log.shape[0], N.ptr(wct), num_wct,
+              N.ptr(fwd.states), N.ptr(fwd.iters), N.ptr(fwd.event_log), fwd.event_log.shape[1], N.ptr(wct), num_wct,
               N.ptr(m), N.ptr(s), N.ptr(q), N.ptr(workspace), int(workspace.numel()), N.ptr(ray_order))
     with torch.cuda.device(device):
         if slot_order is None:
@@ -301,7 +301,7 @@ def reference_tri_collection(scene: Scene, fwd: ForwardResult, max_iters: int, r
     tri = torch.empty(R * int(max_iters), dtype=torch.int32, device=scene.device)
     with torch.cuda.device(scene.device):
         N.check(N.load().ever_event_log_to_reference(ctypes.byref(scene.c), N.ptr(log),
-                                                     0 if log is None else log.shape[0], N.ptr(fwd.iters), R,
+                                                     0 if log is None else log.shape[1], N.ptr(fwd.iters), R,
                                                      N.ptr(ray_order), N.ptr(tri), int(max_iters),
                                                      _stream(scene.device)))
     return tri

@@ -33,7 +33,7 @@ extern "C" {
 #define EVER_ERR_CUDA 2      /* a CUDA launch or API call failed */
 #define EVER_ERR_WORKSPACE 3 /* workspace too small */
 
-#define EVER_ABI_VERSION 1
+#define EVER_ABI_VERSION 2
 
 /* A scene built by ever_scene_build(): a binary LBVH over the ellipsoids plus their
  * intersection records, both in Morton order, all inside the caller's workspace.
@@ -72,10 +72,12 @@ typedef struct EverForwardOut {
   float* states;       /* (R,16) final SplineState (structs.h:41-53 layout); needed by backward */
   float* last_dirac;   /* (R,4) dirac of the last consumed event */
   int32_t* iters;      /* (R) consumed events (required) */
-  int32_t* event_log;  /* (log_cap, R) iteration-major event ids in Morton numbering
-                          (2j+1 entry, 2j exit); column = launch slot (ray ray_order[slot],
-                          or ray slot without ray_order); needed by backward */
-  int32_t log_cap;     /* rows of event_log (>= max_iters to log every event) */
+  int32_t* event_log;  /* (slots, log_cap) ray-major event ids in Morton numbering
+                          (2j+1 entry, 2j exit): row = launch slot (ray ray_order[slot], or
+                          ray slot without ray_order), entries in event order, so a ray's
+                          replay reads consecutive words; needed by backward.
+                          ever_event_log_to_reference gives the reference's layout */
+  int32_t log_cap;     /* entries per row of event_log (>= max_iters to log every event) */
   int32_t* touch_count;/* (N) original order: events per ellipsoid (atomic, exact) */
   float* ray_stats;    /* (R,2): consumed events, termination depth (t of last event) */
   int32_t* status;     /* (1) OR of EVER_STATUS_* flags raised by the kernels */
@@ -275,7 +277,7 @@ int ever_batch_setup(const EverScene* scenes, void* const* bwd_workspaces, int32
 int ever_batch_order(const EverBatch* batch, const float* rayo, const float* rayd, void* stream);
 
 /* One persistent forward launch over all views. Outputs are indexed by ray; event_log
- * has log_cap rows of batch->num_slots columns. The colour follows args->sh_degree as in
+ * has batch->num_slots rows of log_cap entries. The colour follows args->sh_degree as in
  * ever_trace_forward; every scene must hold the coefficients it needs. */
 int ever_trace_forward_batched(const EverBatch* batch, const float* rayo, const float* rayd,
                                const EverTraceArgs* args, const EverTune* tune, const EverForwardOut* out,

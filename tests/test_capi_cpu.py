@@ -32,7 +32,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_workspace_sizes():
     lib = N.load()
-    assert lib.ever_abi_version() == 1
+    assert lib.ever_abi_version() == 2
     a = lib.ever_scene_workspace_bytes(1000, 1)
     b = lib.ever_scene_workspace_bytes(1000, 16)
     assert 0 < a < b
