@@ -205,3 +205,48 @@ def binned_order(rayo: torch.Tensor, rayd: torch.Tensor, bins: torch.Tensor,
     N.check(lib.ever_ray_order_binned(N.ptr(rayo), N.ptr(rayd), N.ptr(bins), R, N.ptr(ws), ws.numel(), N.ptr(order),
                                       ctypes.c_void_p(torch.cuda.current_stream(rayo.device).cuda_stream)))
     return order
+
+
+# ---------------------------------------------------------------------- gating
+def heldout_r2(cm: "CostModel", rayo: torch.Tensor, rayd: torch.Tensor, ray_stats: torch.Tensor,
+               centre=(0.0, 0.0, 0.0), scale: float = 1.0) -> tuple[float, float]:
+    """Coefficient of determination of the model's two outputs (log events, depth) on rays it
+    was not trained on, against the tracer's logs for them."""
+    pred, _ = cm.predict(rayo, rayd)
+    t = cost_targets(ray_stats, rayo, rayd, centre, scale)
+    r2 = []
+    for c in range(2):
+        var = float(t[:, c].var())
+        r2.append(1.0 - float(((pred[:, c] - t[:, c]) ** 2).mean()) / var if var > 0 else float("-inf"))
+    return r2[0], r2[1]
+
+
+class Gate:
+    """Which uses of the model are switched on. A use is on only when the model predicts its
+    target better than a constant on held-out rays (R^2 > 0) and, where a measured speedup
+    against the coherent order alone is given, that speedup is above 1. Otherwise the plain
+    coherent order (and no depth hint) is what runs."""
+
+    def __init__(self, r2_events: float, r2_depth: float, speedup_bins: Optional[float] = None,
+                 speedup_depth: Optional[float] = None):
+        self.bins = r2_events > 0.0 and (speedup_bins is None or speedup_bins > 1.0)
+        self.depth = r2_depth > 0.0 and (speedup_depth is None or speedup_depth > 1.0)
+
+
+def plan(cm: "CostModel", rayo: torch.Tensor, rayd: torch.Tensor, gate: Gate, thresholds=None,
+         centre=(0.0, 0.0, 0.0), scale: float = 1.0, workspace: Optional[torch.Tensor] = None):
+    """(ray_order, depth_hint) for one trace: cost bins only if the gate allows them (with
+    thresholds), the depth hint only if it allows that; the coherent order otherwise."""
+    from . import tracer as T
+    hint = None
+    if gate.bins and thresholds is not None:
+        pred, bins = cm.predict(rayo, rayd, thresholds=thresholds)
+        order = binned_order(rayo, rayd, bins, workspace)
+    else:
+        pred = None
+        order = T.ray_order(rayo, rayd, workspace)
+    if gate.depth:
+        if pred is None:
+            pred, _ = cm.predict(rayo, rayd)
+        hint = depth_from_prediction(pred, rayo, rayd, centre, scale)
+    return order, hint
