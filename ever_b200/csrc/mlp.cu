@@ -37,12 +37,13 @@ namespace ever {
 namespace {
 
 constexpr int kTile = 128;  // rays per tile = MMA M
-constexpr int kK0 = 48;     // encoding columns the first layer reads (39 used)
+constexpr int kK0 = 48;     // first layer's K: the 39 features, a constant 1 (column 39), zeros
+constexpr int kK1 = 80;     // second layer's K: the 64 hidden units, a constant 1 (column 64), zeros
 constexpr int kFeat = 39;
 constexpr int kIn = 64;     // row length of W1 in the parameter block
 constexpr int kHid = 64;
 constexpr int kOut = 16;    // padded output width (2 used)
-constexpr int kOnes = 16;   // columns of the all-ones operand of the bias-gradient products
+constexpr int kOnes = 16;   // columns 64..79 of a hidden tile: the constant-1 column, then zeros
 constexpr int kWorkers = 4;
 constexpr int kMmaWarp = 4 * kWorkers;
 constexpr int kThreads = 32 * (kMmaWarp + 1);
@@ -186,16 +187,9 @@ __device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, float (&v)[32]) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// bf16(relu(a + b)) of two columns, packed (column 2j in the low half): one paired fp32
-// add (each lane rounds as a scalar add) and one converting, clamping cvt. ReLU before
-// or after the rounding gives the same bf16 value.
-__device__ __forceinline__ uint32_t bias_relu_bf16x2(float a0, float a1, float b0, float b1) {
-  uint64_t x, y, z;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(x) : "f"(a0), "f"(a1));
-  asm("mov.b64 %0, {%1, %2};" : "=l"(y) : "f"(b0), "f"(b1));
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(z) : "l"(x), "l"(y));
-  float lo, hi;
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(z));
+// bf16(relu(a)) of two columns, packed (column 2j in the low half): one converting,
+// clamping cvt (the layer's bias is already in the accumulator).
+__device__ __forceinline__ uint32_t relu_bf16x2(float lo, float hi) {
   uint32_t r;
   asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
   return r;
@@ -288,7 +282,9 @@ __device__ __forceinline__ void encode_ray(const MlpParams& P, float ox, float o
     }
   }
 #pragma unroll
-  for (int k = kFeat; k < kK0; ++k) f[k] = 0.f;
+  f[kFeat] = 1.f;  // multiplies the first layer's bias, held in W1's column 39
+#pragma unroll
+  for (int k = kFeat + 1; k < kK0; ++k) f[k] = 0.f;
 #pragma unroll
   for (int j = 0; j < kK0 / 2; ++j) w[j] = pack_bf16x2(f[2 * j], f[2 * j + 1]);
 }
@@ -298,19 +294,19 @@ __device__ __forceinline__ void encode_ray(const MlpParams& P, float ox, float o
 template <bool TRAIN>
 struct WorkerTiles {
   __align__(128) unsigned char a0[kTile * kK0 * 2];  // encoding          [ray][48]
-  __align__(128) unsigned char h1[kTile * kHid * 2];  // hidden 1 / G1     [ray][64]
+  __align__(128) unsigned char h1[kTile * kK1 * 2];  // hidden 1 (and 2)  [ray][80]
 };
 template <>
 struct WorkerTiles<true> {
   __align__(128) unsigned char a0[kTile * kK0 * 2];
-  __align__(128) unsigned char h1[kTile * kHid * 2];
+  __align__(128) unsigned char h1[kTile * kK1 * 2];  // hidden 1 / G1     [ray][80]
   __align__(128) unsigned char h2[kTile * kHid * 2];  // hidden 2 / G2     [ray][64]
   __align__(128) unsigned char g3[kTile * kOut * 2];  // dL/d output       [ray][16]
 };
 
 template <bool TRAIN>
 struct Smem {
-  float b1[kHid], b2[kHid], b3[kOut];
+  float b3[kOut];
   float gb3[kMmaWarp][2], loss[kMmaWarp];  // per worker-warp sums (fixed order)
   uint64_t ready[kWorkers], done[kWorkers];
   int quit[kWorkers];
@@ -318,10 +314,9 @@ struct Smem {
   int abort;   // the MMA warp gave up
   int failed;  // a wait of this CTA ran out
   uint32_t tmem_base;
-  __align__(128) unsigned char w1[kHid * kK0 * 2];   // [h1][48]  K-major, rows = output units
-  __align__(128) unsigned char w2[kHid * kHid * 2];  // [h2][h1]
+  __align__(128) unsigned char w1[kHid * kK0 * 2];   // [h1][48]  K-major, rows = output units; b1 in column 39
+  __align__(128) unsigned char w2[kHid * kK1 * 2];   // [h2][80]: h1, then b2 in column 64
   __align__(128) unsigned char w3[kOut * kHid * 2];  // [out][h2]
-  __align__(128) unsigned char ones[kOnes * kTile * 2];  // training: all-ones [16][128 rays]
   WorkerTiles<TRAIN> t[kWorkers];
 };
 
@@ -366,9 +361,9 @@ __device__ __forceinline__ void issue_step(Smem<TRAIN>& S, uint32_t tmem, int w,
       mma(d, desc_k(sa0, kTile, ks), desc_k(sw1, kHid, ks), idesc(128, kHid, false, false), ks > 0);
     return;
   }
-  if (q == 1) {  // layer 2: D = H1 W2^T
+  if (q == 1) {  // layer 2: D = [H1 1] [W2 b2]^T
 #pragma unroll
-    for (int ks = 0; ks < kHid / 16; ++ks)
+    for (int ks = 0; ks < kK1 / 16; ++ks)
       mma(d, desc_k(sh1, kTile, ks), desc_k(sw2, kHid, ks), idesc(128, kHid, false, false), ks > 0);
     return;
   }
@@ -377,7 +372,9 @@ __device__ __forceinline__ void issue_step(Smem<TRAIN>& S, uint32_t tmem, int w,
     for (int ks = 0; ks < kHid / 16; ++ks)
       mma(d, desc_k(sh1, kTile, ks), desc_k(sw3, kOut, ks), idesc(128, kOut, false, false), ks > 0);
   } else {
-    const uint32_t sh2 = smem_u32(S.t[w].h2), sg3 = smem_u32(S.t[w].g3), sones = smem_u32(S.ones);
+    const uint32_t sh2 = smem_u32(S.t[w].h2), sg3 = smem_u32(S.t[w].g3);
+    // columns 64..79 of h1 (the constant 1, then zeros), read MN-major: a [ray][16] operand
+    const uint32_t sones = sh1 + kmaj(0, kHid, kTile);
     if (q == 2) {  // layer 3
       for (int ks = 0; ks < kHid / 16; ++ks)
         mma(d, desc_k(sh2, kTile, ks), desc_k(sw3, kOut, ks), idesc(128, kOut, false, false), ks > 0);
@@ -398,7 +395,7 @@ __device__ __forceinline__ void issue_step(Smem<TRAIN>& S, uint32_t tmem, int w,
         // dW2[h2][h1] += G2^T A1
         mma(tmem + kColGW2, desc_mn(sh2, kTile, ks), desc_mn(sh1, kTile, ks), idesc(64, kHid, true, true), acc);
         // db2 (every column) += G2^T 1
-        mma(tmem + kColGB2, desc_mn(sh2, kTile, ks), desc_k(sones, kOnes, ks), idesc(64, kOnes, true, false), acc);
+        mma(tmem + kColGB2, desc_mn(sh2, kTile, ks), desc_mn(sones, kTile, ks), idesc(64, kOnes, true, true), acc);
       }
       gs.w2 = true;
     } else {
@@ -406,7 +403,7 @@ __device__ __forceinline__ void issue_step(Smem<TRAIN>& S, uint32_t tmem, int w,
       for (int ks = 0; ks < kTile / 16; ++ks) {
         const uint32_t acc = uint32_t(ks > 0 || gs.w1);
         mma(tmem + kColGW1, desc_mn(sh1, kTile, ks), desc_mn(sa0, kTile, ks), idesc(64, kK0, true, true), acc);
-        mma(tmem + kColGB1, desc_mn(sh1, kTile, ks), desc_k(sones, kOnes, ks), idesc(64, kOnes, true, false), acc);
+        mma(tmem + kColGB1, desc_mn(sh1, kTile, ks), desc_mn(sones, kTile, ks), idesc(64, kOnes, true, true), acc);
       }
       gs.w1 = true;
     }
@@ -431,27 +428,32 @@ __global__ void __launch_bounds__(threads_of<TRAIN>(), 1) k_mlp(const MlpParams 
     const __nv_bfloat16* w1 = static_cast<const __nv_bfloat16*>(P.w1);
     const __nv_bfloat16* w2 = static_cast<const __nv_bfloat16*>(P.w2);
     const __nv_bfloat16* w3 = static_cast<const __nv_bfloat16*>(P.w3);
+    // the hidden layers' biases go into the weight tiles, as bf16, in the column that meets
+    // the operand's constant 1: b1 in W1's column 39, b2 in W2's column 64
+    auto bf16_bits = [](float x) { return uint32_t(__bfloat16_as_ushort(__float2bfloat16_rn(x))); };
     for (int i = tid; i < kHid * kK0 / 8; i += kThreadsT) {
       const int o = i / (kK0 / 8), c0 = (i % (kK0 / 8)) * 8;
-      *reinterpret_cast<uint4*>(S.w1 + kmaj(o, c0, kHid)) = *reinterpret_cast<const uint4*>(w1 + o * kIn + c0);
+      uint4 q = *reinterpret_cast<const uint4*>(w1 + o * kIn + c0);
+      if (c0 == kFeat / 8 * 8) q.w = (q.w & 0xFFFFu) | (bf16_bits(P.params[kOffB1 + o]) << 16);  // column 39
+      *reinterpret_cast<uint4*>(S.w1 + kmaj(o, c0, kHid)) = q;
     }
-    for (int i = tid; i < kHid * kHid / 8; i += kThreadsT) {
-      const int o = i / (kHid / 8), c0 = (i % (kHid / 8)) * 8;
-      *reinterpret_cast<uint4*>(S.w2 + kmaj(o, c0, kHid)) = *reinterpret_cast<const uint4*>(w2 + o * kHid + c0);
+    for (int i = tid; i < kHid * kK1 / 8; i += kThreadsT) {
+      const int o = i / (kK1 / 8), c0 = (i % (kK1 / 8)) * 8;
+      uint4 q = make_uint4(0u, 0u, 0u, 0u);
+      if (c0 < kHid) q = *reinterpret_cast<const uint4*>(w2 + o * kHid + c0);
+      else if (c0 == kHid) q.x = bf16_bits(P.params[kOffB2 + o]);  // column 64
+      *reinterpret_cast<uint4*>(S.w2 + kmaj(o, c0, kHid)) = q;
     }
     for (int i = tid; i < kOut * kHid / 8; i += kThreadsT) {
       const int o = i / (kHid / 8), c0 = (i % (kHid / 8)) * 8;
       *reinterpret_cast<uint4*>(S.w3 + kmaj(o, c0, kOut)) = *reinterpret_cast<const uint4*>(w3 + o * kHid + c0);
     }
-    if (TRAIN) {
-      const uint32_t one2 = 0x3F803F80u;  // two bf16 1.0
-      for (int i = tid; i < kOnes * kTile * 2 / 16; i += kThreadsT)
-        reinterpret_cast<uint4*>(S.ones)[i] = make_uint4(one2, one2, one2, one2);
+    // columns 64..79 of every worker's hidden tile: the constant 1, then zeros (never rewritten)
+    for (int i = tid; i < kWorkers * kTile * 2; i += kThreadsT) {
+      const int w = i / (2 * kTile), row = (i / 2) % kTile, c0 = kHid + 8 * (i & 1);
+      *reinterpret_cast<uint4*>(S.t[w].h1 + kmaj(row, c0, kTile)) =
+          make_uint4(c0 == kHid ? 0x3F80u : 0u, 0u, 0u, 0u);
     }
-  }
-  if (tid < kHid) {
-    S.b1[tid] = P.params[kOffB1 + tid];
-    S.b2[tid] = P.params[kOffB2 + tid];
   }
   if (tid < kOut) S.b3[tid] = P.params[kOffB3 + tid];
   if (tid < kMmaWarp) {
@@ -585,6 +587,7 @@ __global__ void __launch_bounds__(threads_of<TRAIN>(), 1) k_mlp(const MlpParams 
         float f[kK0];
 #pragma unroll
         for (int c = 0; c < kK0; ++c) f[c] = (valid && c < kFeat) ? __ldg(P.feat + r * kIn + c) : 0.f;
+        f[kFeat] = 1.f;
 #pragma unroll
         for (int j = 0; j < kK0 / 2; ++j) enc[j] = pack_bf16x2(f[2 * j], f[2 * j + 1]);
       } else {
@@ -601,12 +604,11 @@ __global__ void __launch_bounds__(threads_of<TRAIN>(), 1) k_mlp(const MlpParams 
       for (int c = 0; c < kK0 / 8; ++c)
         *reinterpret_cast<uint4*>(T.a0 + kmaj(row, 8 * c, kTile)) =
             make_uint4(enc[4 * c], enc[4 * c + 1], enc[4 * c + 2], enc[4 * c + 3]);
-      // ---- layers 1 and 2: bias, ReLU, bf16 into the next operand tile
+      // ---- layers 1 and 2 (biases already in the accumulator): ReLU, bf16 into the next operand tile
 #pragma unroll 1
       for (int layer = 0; layer < 2; ++layer) {
         if (!hand_over(layer)) break;
         await_mma();
-        const float* b = layer == 0 ? S.b1 : S.b2;
         unsigned char* dst = (TRAIN && layer == 1) ? reinterpret_cast<WorkerTiles<true>&>(T).h2 : T.h1;
 #pragma unroll
         for (int half = 0; half < 2; ++half) {  // 32 columns at a time (registers)
@@ -614,11 +616,7 @@ __global__ void __launch_bounds__(threads_of<TRAIN>(), 1) k_mlp(const MlpParams 
           tmem_ld<32>(dcol + 32 * half, v);
           uint32_t h[16];
 #pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const float4 bb = *reinterpret_cast<const float4*>(b + 32 * half + 4 * j);
-            h[2 * j] = bias_relu_bf16x2(v[4 * j], v[4 * j + 1], bb.x, bb.y);
-            h[2 * j + 1] = bias_relu_bf16x2(v[4 * j + 2], v[4 * j + 3], bb.z, bb.w);
-          }
+          for (int j = 0; j < 16; ++j) h[j] = relu_bf16x2(v[2 * j], v[2 * j + 1]);
 #pragma unroll
           for (int c = 0; c < 2; ++c) st16(dst, row, 32 * half + 16 * c, kTile, h + 8 * c);
         }
@@ -717,7 +715,7 @@ __global__ void __launch_bounds__(threads_of<TRAIN>(), 1) k_mlp(const MlpParams 
       if (c0 < kK0) tmem_ld<16>(tmem + lanes + kColGW1 + c0, v);
       if (lane < 16)
 #pragma unroll
-        for (int i = 0; i < 16; ++i) out[kOffW1 + m * kIn + c0 + i] = (any && c0 < kK0) ? v[i] : 0.f;
+        for (int i = 0; i < 16; ++i) out[kOffW1 + m * kIn + c0 + i] = (any && c0 + i < kFeat) ? v[i] : 0.f;
     }
 #pragma unroll
     for (int c0 = 0; c0 < kHid; c0 += 16) {
@@ -814,7 +812,8 @@ static_assert(offsetof(Smem<true>, w1) % 128 == 0 && offsetof(Smem<true>, t) % 1
                   offsetof(Smem<false>, t) % 128 == 0 && sizeof(WorkerTiles<true>) % 128 == 0 &&
                   sizeof(WorkerTiles<false>) % 128 == 0,
               "tiles aligned");
-static_assert(kmaj(127, 63, 128) + 2 == kTile * kHid * 2 && kmaj(127, 47, 128) + 2 == kTile * kK0 * 2,
+static_assert(kmaj(127, 63, 128) + 2 == kTile * kHid * 2 && kmaj(127, 47, 128) + 2 == kTile * kK0 * 2 &&
+                  kmaj(127, 79, 128) + 2 == kTile * kK1 * 2 && kmaj(63, 79, 64) + 2 == kHid * kK1 * 2,
               "tile layout covers the tile");
 static_assert(kThreads <= 1024 && kWorkers <= 15, "block size and named barriers");
 

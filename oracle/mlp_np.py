@@ -4,10 +4,12 @@ and bench.py's CPU baseline, never by the product path).
 The network has no counterpart in the reference. Its specification is the GPU kernel's:
 - input: 39 features of the point of the ray's line closest to the scene centre, zero-padded
   to 64 columns (the kernel reads 48; columns 39.. are zero), rounded to bf16;
-- layers: z1 = A0 W1^T + b1, A1 = bf16(relu(z1)); z2 = A1 W2^T + b2, A2 = bf16(relu(z2));
-  y = A2 W3^T + b3 (outputs 0 and 1 of 16);
-- weights are the bf16 roundings of the fp32 parameters; products are summed in fp64 here
-  and rounded to fp32 before the fp32 bias add, as the tensor cores accumulate in fp32;
+- layers: z1 = A0 W1^T + bf16(b1), A1 = bf16(relu(z1)); z2 = A1 W2^T + bf16(b2),
+  A2 = bf16(relu(z2)); y = A2 W3^T + b3 (outputs 0 and 1 of 16);
+- weights are the bf16 roundings of the fp32 parameters. The hidden layers' biases enter the
+  tensor-core products as bf16 weights against a constant-1 input column, so they are
+  summed with the products (in fp64 here) before the one rounding to fp32; the output bias
+  is added in fp32 after it;
 - loss: mean over the batch of w0 (y0 - t0)^2 + w1 (y1 - t1)^2;
 - backward: G3 = bf16(dL/dy); dA2 = G3 W3, masked by A2 > 0, G2 = bf16(.); dA1 = G2 W2,
   masked by A1 > 0, G1 = bf16(.). Weight gradients are G^T A from the bf16 operands; the
@@ -80,8 +82,8 @@ def forward(params, feat, rounding=True):
     feat = np.array(feat, copy=True)
     feat[:, FEAT:] = 0  # the kernel reads the 39 features only
     a0 = rnd(feat)
-    a1 = rnd(np.maximum(acc(a0.astype(d) @ w1.astype(d).T) + P["b1"], 0))
-    a2 = rnd(np.maximum(acc(a1.astype(d) @ w2.astype(d).T) + P["b2"], 0))
+    a1 = rnd(np.maximum(acc(a0.astype(d) @ w1.astype(d).T + rnd(P["b1"]).astype(d)), 0))
+    a2 = rnd(np.maximum(acc(a1.astype(d) @ w2.astype(d).T + rnd(P["b2"]).astype(d)), 0))
     y = acc(a2.astype(d) @ w3.astype(d).T) + P["b3"]
     return dict(a0=a0, a1=a1, a2=a2, y=y[:, :2], w1=w1, w2=w2, w3=w3)
 
