@@ -242,7 +242,7 @@ int ever_trace_backward_batched(const EverBatch* batch, const float* rayo, const
 }
 
 int ever_scene_finalize_gradients(const EverScene* scene, const float* mean, const float* scale,
-                                  const float* quat, const void* bwd_workspace, size_t bwd_workspace_bytes,
+                                  const float* quat, void* bwd_workspace, size_t bwd_workspace_bytes,
                                   const EverBackwardOut* out, void* stream) {
   if (!scene || !out) return set_last_error(EVER_ERR_INVALID, "ever_scene_finalize_gradients: null pointer");
   const int64_t N = scene->num_prims;
@@ -251,9 +251,10 @@ int ever_scene_finalize_gradients(const EverScene* scene, const float* mean, con
       !out->dfeatures)
     return set_last_error(EVER_ERR_INVALID, "ever_scene_finalize_gradients: null pointer");
   WsCursor c;
-  const char* bw = static_cast<const char*>(bwd_workspace);
+  char* bw = static_cast<char*>(bwd_workspace);
   const int64_t g = c.take(N * 16 * sizeof(float));
   const int64_t f = c.take(N * int64_t(feat_stride(scene->sh_coeffs)) * sizeof(float));
+  const int64_t v = c.take(N * int64_t(sizeof(int32_t)));
   if (bwd_workspace_bytes < size_t(c.offset))
     return set_last_error(EVER_ERR_WORKSPACE, "ever_scene_finalize_gradients: workspace too small");
   FinalizeParams F{};
@@ -266,6 +267,7 @@ int ever_scene_finalize_gradients(const EverScene* scene, const float* mean, con
   F.quat = quat;
   F.acc_geo = reinterpret_cast<const float*>(bw + g);
   F.acc_feat = reinterpret_cast<const float*>(bw + f);
+  F.inv_order = reinterpret_cast<int32_t*>(bw + v);
   F.wct = nullptr;
   F.num_wct = 0;
   F.out = *out;

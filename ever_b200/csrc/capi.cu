@@ -182,6 +182,7 @@ size_t ever_backward_workspace_bytes(int64_t num_prims, int32_t sh_coeffs) {
   ever::WsCursor c;
   c.take(num_prims * 16 * sizeof(float));
   c.take(num_prims * int64_t(ever::feat_stride(sh_coeffs)) * sizeof(float));
+  c.take(num_prims * int64_t(sizeof(int32_t)));  // inverse Morton order for the finalize
   return size_t(c.offset);
 }
 
@@ -221,6 +222,7 @@ int trace_backward(const EverScene* scene, const float* rayo, const float* rayd,
   char* ws = static_cast<char*>(workspace);
   float* acc_geo = reinterpret_cast<float*>(ws + c.take(N * 16 * sizeof(float)));
   float* acc_feat = reinterpret_cast<float*>(ws + c.take(N * int64_t(ever::feat_stride(scene->sh_coeffs)) * sizeof(float)));
+  int32_t* inv_order = reinterpret_cast<int32_t*>(ws + c.take(N * int64_t(sizeof(int32_t))));
   cudaError_t e = cudaSuccess;
   // degree 0 keeps its DC feature gradients in the geometry rows: only those are cleared
   if (N > 0) e = cudaMemsetAsync(workspace, 0, deg == 0 ? size_t(N) * 16 * sizeof(float) : need, st);
@@ -271,6 +273,7 @@ int trace_backward(const EverScene* scene, const float* rayo, const float* rayd,
     F.quat = quat;
     F.acc_geo = acc_geo;
     F.acc_feat = acc_feat;
+    F.inv_order = inv_order;
     F.dc_only = deg == 0;
     F.wct = wct;
     F.num_wct = wct ? num_wct : 0;

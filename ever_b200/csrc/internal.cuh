@@ -217,6 +217,7 @@ struct FinalizeParams {
   const float* quat;
   const float* acc_geo;
   const float* acc_feat;
+  int32_t* inv_order;  // (N) scratch: Morton position of each original index
   bool dc_only;      // degree-0 trace: acc_feat was neither cleared nor written (not read)
   const float* wct;  // first matrix, for the single-camera dmeans2d
   int num_wct;

@@ -724,8 +724,16 @@ __device__ __forceinline__ void rotate_vector_vjp_q(const float v[3], float4 q, 
 
 // Per ellipsoid: W gradients -> scale / quaternion gradients, dmeans2d, clipping
 // (fast_ellipsoid_splinetracer.py:204-219), scatter to original order.
-__global__ void k_finalize(const FinalizeParams P) {
+// Morton position of every original index: inv[order[j]] = j.
+__global__ void k_inverse_order(const int32_t* __restrict__ order, int64_t N, int32_t* __restrict__ inv) {
   const int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (j < N) inv[order[j]] = int32_t(j);
+}
+
+// One thread per ellipsoid in original order (the gradient tensors' order), so the writes
+// are coalesced; it reads its Morton-ordered gradient row and record through inv_order.
+__global__ void k_finalize(const FinalizeParams P) {
+  const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   __shared__ float wct[16], iwct[16];
   const bool single_wct = P.wct && P.num_wct == 1 && P.out.dmeans2d;
   if (single_wct && threadIdx.x == 0) {
@@ -733,9 +741,20 @@ __global__ void k_finalize(const FinalizeParams P) {
     inverse4(wct, iwct);
   }
   __syncthreads();
-  if (j >= P.N) return;
-  const int64_t p = P.order[j];
-  const float* g = P.acc_geo + j * kGeo;
+  if (p >= P.N) return;
+  const int64_t j = P.inv_order[p];
+  float g[kGeo];
+  {
+    const float4* g4 = reinterpret_cast<const float4*>(P.acc_geo + j * kGeo);
+#pragma unroll
+    for (int i = 0; i < kGeo / 4; ++i) {
+      const float4 v = g4[i];
+      g[4 * i] = v.x;
+      g[4 * i + 1] = v.y;
+      g[4 * i + 2] = v.z;
+      g[4 * i + 3] = v.w;
+    }
+  }
   const Record R = load_record(reinterpret_cast<const Record*>(P.records), int(j));
   const float Wm[9] = {R.r0.x, R.r0.y, R.r0.z, R.r1.x, R.r1.y, R.r1.z, R.r2.x, R.r2.y, R.r2.z};
   const float4 q = make_float4(P.quat[4 * p], P.quat[4 * p + 1], P.quat[4 * p + 2], P.quat[4 * p + 3]);
@@ -911,6 +930,7 @@ cudaError_t launch_camera_log_to_reference(const CameraParams& cam, const int32_
 
 cudaError_t launch_finalize(const FinalizeParams& P, cudaStream_t st) {
   if (P.N == 0) return cudaSuccess;
+  k_inverse_order<<<unsigned((P.N + 255) / 256), 256, 0, st>>>(P.order, P.N, P.inv_order);
   k_finalize<<<unsigned((P.N + 255) / 256), 256, 0, st>>>(P);
   const int cols = feat_stride(P.K) / 4, rows = 256 / cols > 0 ? 256 / cols : 1;
   const bool vec = (3 * P.K) % 4 == 0 && reinterpret_cast<uintptr_t>(P.out.dfeatures) % 16 == 0;

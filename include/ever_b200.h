@@ -291,9 +291,10 @@ int ever_trace_backward_batched(const EverBatch* batch, const float* rayo, const
                                 float* drayd, const EverTune* tune, void* stream);
 
 /* Turns one scene's accumulated gradients (its backward workspace) into dmean, dscale,
- * dquat, ddensity, dfeatures (clipped as fast_ellipsoid_splinetracer.py:204-219). */
+ * dquat, ddensity, dfeatures (clipped as fast_ellipsoid_splinetracer.py:204-219). The
+ * workspace's last num_prims int32 are scratch (the inverse Morton order). */
 int ever_scene_finalize_gradients(const EverScene* scene, const float* mean, const float* scale,
-                                  const float* quat, const void* bwd_workspace, size_t bwd_workspace_bytes,
+                                  const float* quat, void* bwd_workspace, size_t bwd_workspace_bytes,
                                   const EverBackwardOut* out, void* stream);
 
 /* ---- learned ray-cost model and cost-binned ray orders ----
