@@ -43,6 +43,16 @@ from torch.autograd import Function
 
 from . import tracer as T
 
+_SIDE_STREAMS: dict = {}
+
+
+def _side_stream(device) -> torch.cuda.Stream:
+    """One side stream per device for work that overlaps the BVH build."""
+    key = torch.device(device).index
+    if key not in _SIDE_STREAMS:
+        _SIDE_STREAMS[key] = torch.cuda.Stream(device)
+    return _SIDE_STREAMS[key]
+
 __all__ = ["SplineTracer", "trace_rays", "SavedForBackward"]
 
 
@@ -89,12 +99,26 @@ class SplineTracer(Function):
                 tune = T.Tune(kbuf=pick.kbuf, block=pick.block, traversal=pick.traversal)
                 if not pick.ordered and isinstance(ray_order, str):
                     ray_order = None
-        scene = T.Scene(mean, scale, quat, density, color)
+        if isinstance(ray_order, str) and ray_order != "auto":
+            raise RuntimeError(f"ray_order must be 'auto', None or an int32 tensor, got {ray_order!r}")
+        if isinstance(ray_order, str) and rayo.shape[0] > 0 and rayo.is_cuda:
+            # the coherent ray order needs only the rays: it runs on a side stream while the
+            # BVH is built on the caller's stream
+            main = torch.cuda.current_stream(rayo.device)
+            side = _side_stream(rayo.device)
+            side.wait_stream(main)
+            with torch.cuda.stream(side):
+                ray_order = T.ray_order(rayo, rayd)
+            rayo.record_stream(side)
+            rayd.record_stream(side)
+            scene = T.Scene(mean, scale, quat, density, color)
+            main.wait_stream(side)
+            ray_order.record_stream(main)
+        else:
+            scene = T.Scene(mean, scale, quat, density, color)
+            if isinstance(ray_order, str):
+                ray_order = None
         needs_grad = any(ctx.needs_input_grad[:7]) or (mean2D is not None and ctx.needs_input_grad[10])
-        if isinstance(ray_order, str):
-            if ray_order != "auto":
-                raise RuntimeError(f"ray_order must be 'auto', None or an int32 tensor, got {ray_order!r}")
-            ray_order = T.ray_order(rayo, rayd) if rayo.shape[0] > 0 else None
         fwd = T.forward(scene, rayo, rayd, tmin, tmax, max_iters, sh_degree,
                         log_events=needs_grad or return_extras, touch_count=return_extras, ray_order=ray_order,
                         tune=tune)
