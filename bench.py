@@ -722,7 +722,7 @@ def main():
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "note": "pinned host inputs copied and the image read back every step, on a copy stream that "
                         "overlaps the next step's compute (two device input buffers)"},
-        "gpu_launches": args.steps * 63,
+        "gpu_launches": args.steps * 64,
         "roofline": roofline,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
