@@ -4,11 +4,16 @@ A 39 -> 64 -> 64 -> 2 ReLU MLP (BF16 weights and activations, FP32 accumulation,
 library's hand-written tcgen05 kernels) predicts each ray's cost from the point of its
 line closest to the scene centre: [log(1 + consumed events), depth offset / scale]. It is
 trained on the tracer's own per-ray logs (forward ray_stats: consumed events and the t
-of the last event). Predicted log-costs are cut into four bins by thresholds taken from
-the training predictions; rays are then ordered bin by bin (costliest first), each bin
-in the coherent direction order, so warps see rays of similar cost and the costliest
-packets start first. The trace's results do not depend on the order (each ray's
-arithmetic is the same in any order); the plain order stays the fallback.
+of the last event). Two uses:
+- cost bins: predicted log-costs are cut into four bins by thresholds taken from the
+  training predictions; rays are ordered bin by bin (costliest first), each bin in the
+  coherent direction order;
+- depth hint: the predicted stopping depth bounds each packet's frustum walk
+  (tracer.forward(depth_hint=...)); a ray that goes on continues in the gather rounds.
+The trace's results depend on neither (each ray's arithmetic is the same in any order and
+with any hint). Gate switches a use on only when the model beats a constant on held-out
+rays (and, when measured, beats the coherent order alone); plan() gives the order and hint
+for one trace, the coherent order and no hint being the fallback.
 
 No counterpart in the reference, whose OptiX launch order is the ray index.
 """
