@@ -9,7 +9,7 @@
 // the cost the tracer logs per ray, [log(1 + consumed events), depth offset / scale].
 //
 // One persistent CTA per SM:
-// - kWorkers worker warpgroups. Each takes its own tiles of 128 rays (the MMA's M): it
+// - worker warpgroups (four for training, kInferWorkers for inference). Each takes its own tiles of 128 rays (the MMA's M): it
 //   encodes a tile into shared memory, and after each layer's MMAs reads the accumulator
 //   from tensor memory (bias, ReLU, bf16) into the next layer's operand tile. The rays of
 //   its next tile are loaded into registers while the current tile's MMAs run.
@@ -44,13 +44,14 @@ constexpr int kIn = 64;     // row length of W1 in the parameter block
 constexpr int kHid = 64;
 constexpr int kOut = 16;    // padded output width (2 used)
 constexpr int kOnes = 16;   // columns 64..79 of a hidden tile: the constant-1 column, then zeros
-constexpr int kWorkers = 4;
-constexpr int kMmaWarp = 4 * kWorkers;
+constexpr int kTrainWorkers = 4;  // shared memory holds four sets of training tiles
+constexpr int kInferWorkers = 5;  // 20 warps: 98.9 us per 2M rays (4: 106.2, 6: 98.1 with spills)
+constexpr int kMmaWarp = 4 * kTrainWorkers;  // training: the warp after the workers'
 constexpr int kThreads = 32 * (kMmaWarp + 1);
 // tensor-memory columns: worker w's layer accumulator at 64 w; training adds the
 // weight- and bias-gradient accumulators (M = 64)
 constexpr uint32_t kColGW1 = 256, kColGW2 = 320, kColGW3 = 384, kColGB1 = 400, kColGB2 = 416;
-constexpr uint32_t kColsInfer = 256, kColsTrain = 512;
+constexpr uint32_t kColsInfer = kInferWorkers <= 4 ? 256 : 512, kColsTrain = 512;
 constexpr int kInferSteps = 3, kTrainSteps = 6;  // MMA requests per tile
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -222,26 +223,16 @@ __device__ __forceinline__ float warp_sum(float t) {
 }
 
 // sin(pi x) and cos(pi x): x = n + r with n the nearest integer and |r| <= 1/2 (exact in
-// float), then the Taylor series of sin(pi r) to r^11 and of cos(pi r) to r^12 in Horner
-// form (truncation below 6e-8 on |r| <= 1/2), and the sign (-1)^n.
-__device__ __forceinline__ void sincospi_series(float x, float& s, float& c) {
+// float), the hardware sine and cosine of pi r (|pi r| <= pi/2, absolute error about
+// 2^-21), and the sign (-1)^n.
+__device__ __forceinline__ void sincospi_reduced(float x, float& s, float& c) {
   const float n = rintf(x);
   const float r = x - n;
-  const float r2 = r * r;
-  float ps = fmaf(r2, -0.007370430945714348f, 0.08214588661112819f);
-  ps = fmaf(r2, ps, -0.5992645293207919f);
-  ps = fmaf(r2, ps, 2.550164039877345f);
-  ps = fmaf(r2, ps, -5.167712780049969f);
-  ps = fmaf(r2, ps, 3.141592653589793f);
-  float pc = fmaf(r2, 0.001929574309403922f, -0.02580689139001405f);
-  pc = fmaf(r2, pc, 0.23533063035889312f);
-  pc = fmaf(r2, pc, -1.3352627688545893f);
-  pc = fmaf(r2, pc, 4.058712126416768f);
-  pc = fmaf(r2, pc, -4.934802200544679f);
-  pc = fmaf(r2, pc, 1.f);
+  float ps, pc;
+  __sincosf(3.14159265358979f * r, &ps, &pc);
   // |x| < 2^24 here (larger inputs are already integers: r = 0); the parity of n flips both
   const uint32_t flip = (uint32_t(int(fminf(fabsf(n), 16777216.f))) & 1u) << 31;
-  s = __uint_as_float(__float_as_uint(r * ps) ^ flip);
+  s = __uint_as_float(__float_as_uint(ps) ^ flip);
   c = __uint_as_float(__float_as_uint(pc) ^ flip);
 }
 
@@ -261,14 +252,14 @@ __device__ __forceinline__ void encode_ray(const MlpParams& P, float ox, float o
 #pragma unroll
   for (int i = 0; i < 3; ++i) x[i] = isfinite(x[i]) ? x[i] : 0.f;
   float f[kK0];
-  // sin / cos of 2^q pi x from the series at the lowest frequency and the double-angle
+  // sin / cos of 2^q pi x from the reduced sincos at the lowest frequency and the double-angle
   // identities sin 2a = 2 sin a cos a, cos 2a = 1 - 2 sin^2 a (after five doublings the
   // error is a few 1e-6, far below the bf16 rounding the features go through)
   float sv[3], cv[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
     f[i] = x[i];
-    sincospi_series(x[i], sv[i], cv[i]);
+    sincospi_reduced(x[i], sv[i], cv[i]);
   }
 #pragma unroll
   for (int q = 0; q < 6; ++q) {
@@ -276,8 +267,9 @@ __device__ __forceinline__ void encode_ray(const MlpParams& P, float ox, float o
     for (int i = 0; i < 3; ++i) {
       f[3 + 6 * q + i] = sv[i];
       f[6 + 6 * q + i] = cv[i];
-      const float s2 = 2.f * sv[i] * cv[i];
-      cv[i] = fmaf(-2.f * sv[i], sv[i], 1.f);
+      const float t = 2.f * sv[i];  // exact
+      const float s2 = t * cv[i];
+      cv[i] = fmaf(-t, sv[i], 1.f);
       sv[i] = s2;
     }
   }
@@ -308,16 +300,16 @@ template <bool TRAIN>
 struct Smem {
   float b3[kOut];
   float gb3[kMmaWarp][2], loss[kMmaWarp];  // per worker-warp sums (fixed order)
-  uint64_t ready[kWorkers], done[kWorkers];
-  int quit[kWorkers];
-  int wfail[kWorkers];  // a wait of worker w ran out: its warpgroup stops at its next barrier
+  uint64_t ready[TRAIN ? kTrainWorkers : kInferWorkers], done[TRAIN ? kTrainWorkers : kInferWorkers];
+  int quit[TRAIN ? kTrainWorkers : kInferWorkers];
+  int wfail[TRAIN ? kTrainWorkers : kInferWorkers];  // a wait of worker w ran out: it stops at its next barrier
   int abort;   // the MMA warp gave up
   int failed;  // a wait of this CTA ran out
   uint32_t tmem_base;
   __align__(128) unsigned char w1[kHid * kK0 * 2];   // [h1][48]  K-major, rows = output units; b1 in column 39
   __align__(128) unsigned char w2[kHid * kK1 * 2];   // [h2][80]: h1, then b2 in column 64
   __align__(128) unsigned char w3[kOut * kHid * 2];  // [out][h2]
-  WorkerTiles<TRAIN> t[kWorkers];
+  WorkerTiles<TRAIN> t[TRAIN ? kTrainWorkers : kInferWorkers];
 };
 
 struct RayIn {
@@ -339,7 +331,7 @@ __device__ __forceinline__ RayIn load_ray(const MlpParams& P, int64_t s) {
 // Threads of a CTA: the worker warpgroups, and for training the MMA warp.
 template <bool TRAIN>
 __host__ __device__ constexpr int threads_of() {
-  return TRAIN ? kThreads : 32 * kMmaWarp;
+  return TRAIN ? kThreads : 32 * 4 * kInferWorkers;
 }
 
 // Which accumulators of the CTA's weight and bias gradients hold a sum already (the first
@@ -415,6 +407,7 @@ __device__ __forceinline__ void issue_step(Smem<TRAIN>& S, uint32_t tmem, int w,
 template <bool TRAIN>
 __global__ void __launch_bounds__(threads_of<TRAIN>(), 1) k_mlp(const MlpParams P) {
   constexpr int kThreadsT = threads_of<TRAIN>();
+  constexpr int kWorkers = TRAIN ? kTrainWorkers : kInferWorkers;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   Smem<TRAIN>& S = *reinterpret_cast<Smem<TRAIN>*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -806,7 +799,7 @@ constexpr size_t kInferSmem = sizeof(Smem<false>) + 128;
 constexpr size_t kTrainSmem = sizeof(Smem<true>) + 128;
 static_assert(kTrainSmem <= 227 * 1024, "training shared memory");
 static_assert(kInferSmem <= 227 * 1024, "inference shared memory");
-static_assert(kWorkers * 64 <= int(kColsInfer) && kColGB2 + kOnes <= kColsTrain && kWorkers * 64 <= int(kColGW1),
+static_assert(kInferWorkers * 64 <= int(kColsInfer) && kColGB2 + kOnes <= kColsTrain && kTrainWorkers * 64 <= int(kColGW1),
               "tensor-memory columns");
 static_assert(offsetof(Smem<true>, w1) % 128 == 0 && offsetof(Smem<true>, t) % 128 == 0 &&
                   offsetof(Smem<false>, t) % 128 == 0 && sizeof(WorkerTiles<true>) % 128 == 0 &&
@@ -815,7 +808,7 @@ static_assert(offsetof(Smem<true>, w1) % 128 == 0 && offsetof(Smem<true>, t) % 1
 static_assert(kmaj(127, 63, 128) + 2 == kTile * kHid * 2 && kmaj(127, 47, 128) + 2 == kTile * kK0 * 2 &&
                   kmaj(127, 79, 128) + 2 == kTile * kK1 * 2 && kmaj(63, 79, 64) + 2 == kHid * kK1 * 2,
               "tile layout covers the tile");
-static_assert(kThreads <= 1024 && kWorkers <= 15, "block size and named barriers");
+static_assert(kThreads <= 1024 && 128 * kInferWorkers <= 1024 && kInferWorkers <= 15, "block size and named barriers");
 
 }  // namespace
 
@@ -823,7 +816,7 @@ int mlp_grid(int64_t num_samples, int max_grid, bool train) {
   const int64_t ntiles = (num_samples + kTile - 1) / kTile;
   // training: two tiles per worker, so the warpgroups of a CTA overlap their steps; inference:
   // every SM, as many tiles per worker as it takes
-  const int64_t per_cta = train ? 2 * kWorkers : kWorkers;
+  const int64_t per_cta = train ? 2 * kTrainWorkers : kInferWorkers;
   return int(std::max<int64_t>(1, std::min<int64_t>((ntiles + per_cta - 1) / per_cta, max_grid)));
 }
 
