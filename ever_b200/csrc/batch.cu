@@ -54,11 +54,11 @@ EverTune tune_of(const EverTune* t) {
 
 // Persistent grid: enough resident blocks to fill every SM. Occupancy is bounded by
 // registers: 20 warps per SM for the forward with blocks of 64 or 128 threads, 16 warps
-// otherwise (the backward, and the forward with 256 threads).
-int persistent_grid(int block, bool forward) {
+// with 256 threads; 24 warps for the degree-0 backward, 16 with SH colour.
+int persistent_grid(int block, bool forward, int deg = 0) {
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int warps_per_sm = forward && block <= 128 ? 20 : 16;
+  const int warps_per_sm = forward ? (block <= 128 ? 20 : 16) : (deg == 0 ? 24 : 16);
   return std::max(1, sms * std::max(1, warps_per_sm * 32 / block));
 }
 
@@ -229,7 +229,7 @@ int ever_trace_backward_batched(const EverBatch* batch, const float* rayo, const
   P.drayo = drayo;
   P.drayd = drayd;
   P.work_counter = batch->counters + 1;
-  P.grid = persistent_grid(tn.block, false);
+  P.grid = persistent_grid(tn.block, false, deg);
   // replay order: inside each view, slots grouped by their rays' event counts (longest first)
   char* scratch = static_cast<char*>(batch->order_scratch);
   int32_t* slots = reinterpret_cast<int32_t*>(scratch + ray_order_workspace(std::max<int64_t>(batch->num_slots, 1)));
