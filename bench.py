@@ -696,8 +696,8 @@ def main():
     # kernels) from one single-pass ncu capture of `bench.py --once` on this default workload
     # (1M ellipsoids, 1920x1080): forward = the three passes of the regrouped forward,
     # backward = k_trace_bwd
-    measured_traffic = {"fwd": 252_640_000 + 418_240_000 + 7_440_000 + 9_220 + 33_540,
-                        "bwd": 1_110_000_000 + 109_970_000}
+    measured_traffic = {"fwd": 253_090_000 + 418_550_000 + 7_410_000 + 6_400 + 33_540,
+                        "bwd": 1_180_000_000 + 144_010_000}
     default_workload = args.prims == 1_000_000 and args.width == 1920 and args.height == 1080
     roofline = {"bound": "hbm",
                 "kernel": "k_trace_bwd" if dom == "bwd" else "regrouped forward (k_trace_fwd_pass x3, one library call)",
