@@ -72,6 +72,8 @@ SIGNATURES = {
     "ever_scene_workspace_bytes": (c_sz, [c_i64, c_i32]),
     "ever_scene_build": (ctypes.c_int, [c_p, c_p, c_p, c_p, c_p, c_i64, c_i32, c_p, c_sz,
                                         ctypes.POINTER(EverScene), c_p]),
+    "ever_scene_build_dc": (ctypes.c_int, [c_p, c_p, c_p, c_p, c_p, c_i64, c_i32, c_p, c_sz,
+                                        ctypes.POINTER(EverScene), c_p]),
     "ever_scene_refit": (ctypes.c_int, [c_p, c_p, c_p, c_p, c_p, c_p, c_sz, ctypes.POINTER(EverScene), c_p]),
     "ever_scene_set_features": (ctypes.c_int, [ctypes.POINTER(EverScene), c_p, c_p]),
     "ever_trace_forward": (ctypes.c_int, [ctypes.POINTER(EverScene), c_p, c_p, c_i64, ctypes.POINTER(EverTraceArgs),

@@ -45,6 +45,8 @@ int resolve_degree(const EverScene* sc, const EverTraceArgs* a, int* deg) {
   if ((d + 1) * (d + 1) > sc->sh_coeffs)
     return fail(EVER_ERR_INVALID, "sh_degree %d needs %d SH coefficients, features have %d", d, (d + 1) * (d + 1),
                 sc->sh_coeffs);
+  if (d > 0 && sc->num_prims > 0 && !sc->features)
+    return fail(EVER_ERR_INVALID, "sh_degree %d needs the feature rows; the scene was built with ever_scene_build_dc", d);
   *deg = d;
   return EVER_OK;
 }
@@ -64,9 +66,9 @@ size_t ever_scene_workspace_bytes(int64_t num_prims, int32_t sh_coeffs) {
   return size_t(ever::scene_layout(num_prims, sh_coeffs).total);
 }
 
-int ever_scene_build(const float* mean, const float* scale, const float* quat, const float* density,
-                     const float* features, int64_t num_prims, int32_t sh_coeffs, void* workspace,
-                     size_t workspace_bytes, EverScene* scene, void* stream) {
+static int build_scene(const float* mean, const float* scale, const float* quat, const float* density,
+                       const float* features, int64_t num_prims, int32_t sh_coeffs, void* workspace,
+                       size_t workspace_bytes, EverScene* scene, void* stream, bool dc_only) {
   if (!scene) return fail(EVER_ERR_INVALID, "scene is null");
   if (num_prims < 0 || num_prims >= (int64_t(1) << 30))
     return fail(EVER_ERR_INVALID, "num_prims %lld out of range [0, 2^30)", (long long)num_prims);
@@ -78,8 +80,22 @@ int ever_scene_build(const float* mean, const float* scale, const float* quat, c
     return fail(EVER_ERR_WORKSPACE, "scene workspace needs %lld bytes, got %zu", (long long)L.total, workspace_bytes);
   if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0) return fail(EVER_ERR_INVALID, "workspace not 256-byte aligned");
   cudaError_t e = ever::scene_build(mean, scale, quat, density, features, num_prims, sh_coeffs,
-                                    static_cast<char*>(workspace), L, scene, static_cast<cudaStream_t>(stream));
-  return cuda_status(e, "ever_scene_build");
+                                    static_cast<char*>(workspace), L, scene, static_cast<cudaStream_t>(stream), dc_only);
+  return cuda_status(e, dc_only ? "ever_scene_build_dc" : "ever_scene_build");
+}
+
+int ever_scene_build(const float* mean, const float* scale, const float* quat, const float* density,
+                     const float* features, int64_t num_prims, int32_t sh_coeffs, void* workspace,
+                     size_t workspace_bytes, EverScene* scene, void* stream) {
+  return build_scene(mean, scale, quat, density, features, num_prims, sh_coeffs, workspace, workspace_bytes, scene,
+                     stream, false);
+}
+
+int ever_scene_build_dc(const float* mean, const float* scale, const float* quat, const float* density,
+                        const float* features, int64_t num_prims, int32_t sh_coeffs, void* workspace,
+                        size_t workspace_bytes, EverScene* scene, void* stream) {
+  return build_scene(mean, scale, quat, density, features, num_prims, sh_coeffs, workspace, workspace_bytes, scene,
+                     stream, true);
 }
 
 int ever_scene_set_features(EverScene* scene, const float* features, void* stream) {

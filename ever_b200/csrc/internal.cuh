@@ -49,9 +49,10 @@ cudaError_t ray_order(const float* rayo, const float* rayd, int64_t R, char* ws,
 cudaError_t backward_slot_order(const int32_t* iters, const int32_t* ray_order, int64_t R, int shift, char* ws,
                                 int32_t* slot_order, cudaStream_t st, const BatchView* views = nullptr,
                                 int num_views = 0);
+// dc_only: the scene keeps only each record's DC colour, no feature rows (sc->features null).
 cudaError_t scene_build(const float* mean, const float* scale, const float* quat, const float* density,
                         const float* feat, int64_t N, int K, char* ws, const SceneLayout& L, EverScene* sc,
-                        cudaStream_t st);
+                        cudaStream_t st, bool dc_only = false);
 cudaError_t scene_set_features(EverScene* sc, const float* feat, cudaStream_t st);
 cudaError_t scene_refit(const float* mean, const float* scale, const float* quat, const float* density,
                         const float* feat, char* ws, const SceneLayout& L, EverScene* sc, cudaStream_t st);

@@ -461,8 +461,25 @@ __global__ void k_single_leaf(Node* nodes, const float4* aabb) {
 
 inline int64_t div_up(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Only the records' DC colour C0 * f0 + 0.5 (r3.yzw), for scenes that keep no feature rows:
+// the same bits as k_gather_features' column 0.
+__global__ void k_gather_dc(const int32_t* __restrict__ order, int64_t N, int K, const float* __restrict__ feat,
+                            Record* __restrict__ recs) {
+  const int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (j >= N) return;
+  const float* src = feat + int64_t(__ldg(order + j)) * (3 * K);
+  recs[j].r3.y = dc_channel(__ldg(src));
+  recs[j].r3.z = dc_channel(__ldg(src + 1));
+  recs[j].r3.w = dc_channel(__ldg(src + 2));
+}
+
+// feat_out null: the scene keeps the DC colour only (ever_scene_build_dc).
 void launch_gather_features(const int32_t* order, int64_t N, int K, const float* feat, float* feat_out, void* recs,
                             cudaStream_t st) {
+  if (!feat_out) {
+    k_gather_dc<<<unsigned(div_up(N, 256)), 256, 0, st>>>(order, N, K, feat, static_cast<Record*>(recs));
+    return;
+  }
   const int cols = feat_stride(K) / 4, rows = std::max(1, 256 / cols);
   const bool vec = (3 * K) % 4 == 0 && reinterpret_cast<uintptr_t>(feat) % 16 == 0;
   k_gather_features<<<unsigned(div_up(N, rows)), dim3(cols, rows), 0, st>>>(order, N, K, feat, feat_out,
@@ -518,13 +535,13 @@ SceneLayout scene_layout(int64_t N, int K) {
 
 cudaError_t scene_build(const float* mean, const float* scale, const float* quat, const float* density,
                         const float* feat, int64_t N, int K, char* ws, const SceneLayout& L, EverScene* sc,
-                        cudaStream_t st) {
+                        cudaStream_t st, bool dc_only) {
   sc->num_prims = N;
   sc->sh_coeffs = K;
   sc->num_nodes = N > 0 ? int32_t(N > 1 ? N - 1 : 1) : 0;
   sc->nodes = ws + L.nodes;
   sc->records = ws + L.records;
-  sc->features = reinterpret_cast<float*>(ws + L.features);
+  sc->features = dc_only ? nullptr : reinterpret_cast<float*>(ws + L.features);
   sc->order = reinterpret_cast<int32_t*>(ws + L.order);
   sc->scratch = ws + L.aabb_a;
   if (N == 0) return cudaGetLastError();

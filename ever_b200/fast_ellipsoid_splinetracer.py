@@ -111,11 +111,11 @@ class SplineTracer(Function):
                 ray_order = T.ray_order(rayo, rayd)
             rayo.record_stream(side)
             rayd.record_stream(side)
-            scene = T.Scene(mean, scale, quat, density, color)
+            scene = T.Scene(mean, scale, quat, density, color, dc_only=not sh_degree)
             main.wait_stream(side)
             ray_order.record_stream(main)
         else:
-            scene = T.Scene(mean, scale, quat, density, color)
+            scene = T.Scene(mean, scale, quat, density, color, dc_only=not sh_degree)
             if isinstance(ray_order, str):
                 ray_order = None
         needs_grad = any(ctx.needs_input_grad[:7]) or (mean2D is not None and ctx.needs_input_grad[10])

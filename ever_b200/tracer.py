@@ -54,7 +54,9 @@ class Scene:
     on the device with no host synchronisation. Keeps references to the input tensors.
     """
 
-    def __init__(self, mean, scale, quat, density, features):
+    def __init__(self, mean, scale, quat, density, features, dc_only: bool = False):
+        """dc_only: keep only each ellipsoid's DC colour (ever_scene_build_dc); traces of
+        sh_degree > 0 on the scene are then refused."""
         device = mean.device
         _check_tensor("means", mean, device, 3)
         _check_tensor("scales", scale, device, 3)
@@ -73,15 +75,16 @@ class Scene:
         self.tensors = tuple(t.contiguous() for t in (mean, scale, quat, density, features))
         self.num_prims = n
         self.sh_coeffs = features.shape[1]
+        self.dc_only = bool(dc_only)
         lib = N.load()
         nbytes = lib.ever_scene_workspace_bytes(n, self.sh_coeffs)
         self.workspace = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
         self.c = N.EverScene()
         m, s, q, d, f = self.tensors
         with torch.cuda.device(device):
-            N.check(lib.ever_scene_build(N.ptr(m), N.ptr(s), N.ptr(q), N.ptr(d), N.ptr(f), n, self.sh_coeffs,
-                                         N.ptr(self.workspace), int(self.workspace.numel()), ctypes.byref(self.c),
-                                         _stream(device)))
+            build = lib.ever_scene_build_dc if self.dc_only else lib.ever_scene_build
+            N.check(build(N.ptr(m), N.ptr(s), N.ptr(q), N.ptr(d), N.ptr(f), n, self.sh_coeffs,
+                          N.ptr(self.workspace), int(self.workspace.numel()), ctypes.byref(self.c), _stream(device)))
 
     def rebuild(self):
         """Rebuilds the BVH and records in place from the (possibly updated) input tensors.
@@ -91,9 +94,11 @@ class Scene:
         """
         m, s, q, d, f = self.tensors
         with torch.cuda.device(self.device):
-            N.check(N.load().ever_scene_build(N.ptr(m), N.ptr(s), N.ptr(q), N.ptr(d), N.ptr(f), self.num_prims,
-                                              self.sh_coeffs, N.ptr(self.workspace), int(self.workspace.numel()),
-                                              ctypes.byref(self.c), _stream(self.device)))
+            lib = N.load()
+            build = lib.ever_scene_build_dc if self.dc_only else lib.ever_scene_build
+            N.check(build(N.ptr(m), N.ptr(s), N.ptr(q), N.ptr(d), N.ptr(f), self.num_prims, self.sh_coeffs,
+                          N.ptr(self.workspace), int(self.workspace.numel()), ctypes.byref(self.c),
+                          _stream(self.device)))
 
     def refit(self, with_features=True):
         """Refits the BVH in place to the (updated) input tensors, keeping the last build's

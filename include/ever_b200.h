@@ -128,6 +128,17 @@ int ever_scene_build(const float* mean, const float* scale, const float* quat, c
                      const float* features, int64_t num_prims, int32_t sh_coeffs, void* workspace,
                      size_t workspace_bytes, EverScene* scene, void* stream);
 
+/* ever_scene_build for traces that use the DC colour only (sh_degree 0 / the default, the
+ * reference forward's colour): every record gets its DC colour C0 * f0 + 0.5 from
+ * `features`, but the feature rows are not copied into the workspace (scene->features is
+ * NULL). A trace with sh_degree > 0 on such a scene fails with EVER_ERR_INVALID;
+ * ever_scene_set_features and ever_scene_refit update the DC colours. Same workspace as
+ * ever_scene_build. No counterpart in the reference (its GAS build copies every
+ * feature); trace_rays uses it at its default colour. */
+int ever_scene_build_dc(const float* mean, const float* scale, const float* quat, const float* density,
+                        const float* features, int64_t num_prims, int32_t sh_coeffs, void* workspace,
+                        size_t workspace_bytes, EverScene* scene, void* stream);
+
 /* Replaces the features of a built scene (same N and K) without rebuilding the BVH.
  * Counterpart of Primitives.set_features + Forward.update_model (py_binding.cpp:133-138, 207-209). */
 int ever_scene_set_features(EverScene* scene, const float* features, void* stream);
